@@ -1,0 +1,613 @@
+/*
+ * api.cu — the handle API of libgslam (include/gslam.h).
+ *
+ * A gslam_graph owns one stream and every device buffer of one pose graph. The
+ * symbolic work (edge order, block pattern, layout, contribution lists) runs
+ * once on the host at creation; every round after that is device-only:
+ *   linearise -> assemble -> block-Jacobi inverse -> persistent PCG -> update,
+ * with one 8-byte (diff) and one 40-byte (solver status) read back per round.
+ * The reference rebuilds edges, structure and a 2.3 GB edge array every round
+ * (src/cpu_pcg_fp64/GSLAM.c:55-139) and its GPU twin re-uploads poses and
+ * downloads dx every round (src/gpu_pcg_fp64/device_graph.cu:1060-1129, :911).
+ */
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gslam.h"
+#include "gslam_api_internal.h"
+#include "gslam_internal.h"
+#include "kernels.cuh"
+
+static thread_local std::string g_last_error;
+
+void gslam_set_error(const char *fmt, const char *what, int code) {
+    char buf[512];
+    snprintf(buf, sizeof buf, fmt, what, code);
+    g_last_error = buf;
+}
+
+#define CK(call)                                                                 \
+    do {                                                                         \
+        cudaError_t _e = (call);                                                 \
+        if (_e != cudaSuccess) {                                                 \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(_e);   \
+            return GSLAM_ERR_CUDA;                                               \
+        }                                                                        \
+    } while (0)
+
+#define BAD(msg)                         \
+    do {                                 \
+        g_last_error = (msg);            \
+        return GSLAM_ERR_BAD_INPUT;      \
+    } while (0)
+
+void gslam_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
+const char *gslam_version(void) { return "gslam-b200 0.1 (sm_100a)"; }
+const char *gslam_last_error(void) { return g_last_error.c_str(); }
+
+int gslam_opts_default(gslam_opts *o) {
+    if (!o) return GSLAM_ERR_BAD_INPUT;
+    memset(o, 0, sizeof *o);
+    o->precision = GSLAM_PREC_FP64;
+    o->tol = 1e-6;
+    o->max_iter = 500;
+    o->sell_window = 0;
+    o->threads_per_cta = 0;
+    o->ctas_per_sm = 0;
+    o->angle_wrap = 0;
+    o->inner_tol = 1e-4;
+    o->inner_max_iter = 4000;
+    o->max_refine = 64;
+    o->device = -1;
+    o->barrier_timeout_ms = 0.0;
+    o->test_absent_cta = -1;
+    return GSLAM_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* device buffers                                                            */
+/* ------------------------------------------------------------------------ */
+
+template <class T>
+static cudaError_t dalloc(DevMem &m, T **p, size_t n) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    m.ptrs.push_back(q);
+    *p = (T *)q;
+    return cudaSuccess;
+}
+
+template <class T>
+static cudaError_t dupload(DevMem &m, cudaStream_t st, T **p, const std::vector<T> &v) {
+    cudaError_t e = dalloc(m, p, v.size());
+    if (e != cudaSuccess) return e;
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+void DevMem::release() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+}
+
+int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st, int device,
+                        const gslam_opts &o) {
+    DevMem &m = L->mem;
+    L->n_rows = S.n_rows;
+    L->n_slices = S.n_slices;
+    L->n_slots = S.n_slots;
+    CK(dupload(m, st, &L->perm, S.perm));
+    CK(dupload(m, st, &L->iperm, S.iperm));
+    CK(dupload(m, st, &L->row_len, S.row_len));
+    CK(dupload(m, st, &L->col, S.col));
+    CK(dupload(m, st, &L->diag_slot, S.diag_slot));
+    CK(dupload(m, st, &L->chunk_slice, S.chunk_slice));
+    CK(dupload(m, st, &L->slice_ptr, S.slice_ptr));
+    CK(dupload(m, st, &L->slot_csr, S.slot_csr));
+    const size_t nv = 9 * (size_t)S.n_slots;
+    CK(dalloc(m, &L->val, nv));
+    CK(cudaMemsetAsync(L->val, 0, nv * sizeof(double), st));
+    L->val32 = nullptr;
+    const size_t nr32 = 32 * (size_t)S.n_slices;
+    CK(dalloc(m, &L->dinv, 9 * nr32));
+    const size_t nvec = 4 * nr32;
+    CK(dalloc(m, &L->b4, nvec));
+    CK(dalloc(m, &L->x4, nvec));
+    CK(dalloc(m, &L->r4, nvec));
+    CK(dalloc(m, &L->z4, nvec));
+    CK(dalloc(m, &L->p4a, nvec));
+    CK(dalloc(m, &L->p4b, nvec));
+    CK(dalloc(m, &L->q4, nvec));
+    CK(cudaMemsetAsync(L->b4, 0, nvec * sizeof(double), st));
+    CK(cudaMemsetAsync(L->x4, 0, nvec * sizeof(double), st));
+    for (int i = 0; i < 6; i++) L->f[i] = nullptr;
+    /* solver launch shape */
+    int n_sm = 0;
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
+    L->block = o.threads_per_cta ? o.threads_per_cta : 256;
+    int maxg = pcg_max_grid(GSLAM_PREC_FP64, L->block, device);
+    if (maxg <= 0) {
+        g_last_error = "persistent solver cannot be made co-resident at this block size";
+        return GSLAM_ERR_NO_DEVICE;
+    }
+    int cps = o.ctas_per_sm ? o.ctas_per_sm : 1;
+    int grid = std::min(maxg, cps * n_sm);
+    int warps = L->block / 32;
+    int needed = (S.n_slices + warps - 1) / warps;
+    L->grid = std::max(1, std::min(grid, needed));
+    L->n_sm = n_sm;
+    L->partial_capacity = std::max(L->grid, maxg);
+    CK(dalloc(m, &L->partials, 8 * (size_t)L->partial_capacity));
+    CK(dalloc(m, &L->gs, 1));
+    CK(dalloc(m, &L->res, 1));
+    return GSLAM_OK;
+}
+
+int gslam_layout_ensure_fp32(DevLayout *L, cudaStream_t st) {
+    if (L->val32) return GSLAM_OK;
+    DevMem &m = L->mem;
+    const size_t nv = 9 * (size_t)L->n_slots;
+    CK(dalloc(m, &L->val32, nv));
+    CK(cudaMemsetAsync(L->val32, 0, nv * sizeof(float), st));
+    const size_t nvec = 4 * 32 * (size_t)L->n_slices;
+    for (int i = 0; i < 6; i++) {
+        CK(dalloc(m, &L->f[i], nvec));
+        CK(cudaMemsetAsync(L->f[i], 0, nvec * sizeof(float), st));
+    }
+    return GSLAM_OK;
+}
+
+/* Runs the persistent solver on L->val / L->b4; result in L->x4 (new order). */
+int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgResult *h_res,
+                       gslam_solve_stats *stats) {
+    const int fused_prec = o.precision;
+    if (fused_prec == GSLAM_PREC_MIXED) {
+        int rc = gslam_layout_ensure_fp32(L, st);
+        if (rc != GSLAM_OK) return rc;
+    }
+    launch_diag_inv(st, L->n_rows, L->diag_slot, L->val, L->dinv);
+    CK(cudaGetLastError());
+    PcgParams P;
+    memset(&P, 0, sizeof P);
+    P.n_rows = L->n_rows;
+    P.n_slices = L->n_slices;
+    P.slice_ptr = L->slice_ptr;
+    P.row_len = L->row_len;
+    P.col = L->col;
+    P.val = L->val;
+    P.val32 = L->val32;
+    P.dinv = L->dinv;
+    P.b4 = L->b4;
+    P.x4 = L->x4; P.r4 = L->r4; P.z4 = L->z4; P.p4a = L->p4a; P.p4b = L->p4b; P.q4 = L->q4;
+    P.xf4 = L->f[0]; P.rf4 = L->f[1]; P.zf4 = L->f[2]; P.pfa4 = L->f[3]; P.pfb4 = L->f[4]; P.qf4 = L->f[5];
+    P.tol_rel = o.tol;
+    P.max_iter = o.max_iter;
+    P.inner_tol = o.inner_tol;
+    P.inner_max_iter = o.inner_max_iter;
+    P.max_refine = o.max_refine;
+    P.partials = L->partials;
+    P.gs = L->gs;
+    P.res = L->res;
+    {
+        /* barrier wait limit in SM clock cycles */
+        int khz = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev);
+        if (khz <= 0) khz = 2000000;
+        const double ms = o.barrier_timeout_ms > 0 ? o.barrier_timeout_ms : 2000.0;
+        P.spin_limit = (long long)(ms * (double)khz);
+    }
+    P.absent_cta = o.test_absent_cta;
+    CK(cudaMemsetAsync(L->gs, 0, sizeof(GridSync), st));
+    CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
+    CK(launch_pcg(st, P, fused_prec, L->grid, L->block));
+    CK(cudaMemcpyAsync(h_res, L->res, sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (stats) {
+        stats->iterations = h_res->iterations;
+        stats->refinements = h_res->refinements;
+        stats->reason = h_res->reason;
+        stats->rel_residual = h_res->bnorm > 0 ? h_res->rnorm / h_res->bnorm : 0.0;
+    }
+    if (h_res->timeout) {
+        g_last_error = "solver barrier wait timed out";
+        return GSLAM_ERR_DEVICE_TIMEOUT;
+    }
+    return GSLAM_OK;
+}
+
+void gslam_layout_release(DevLayout *L) { L->mem.release(); }
+
+/* ------------------------------------------------------------------------ */
+/* graph creation                                                            */
+/* ------------------------------------------------------------------------ */
+
+static int common_setup(gslam_graph *g, const gslam_opts *opts) {
+    if (opts) g->o = *opts; else gslam_opts_default(&g->o);
+    if (g->o.sell_window <= 0) g->o.sell_window = 256;
+    if (g->o.device >= 0) CK(cudaSetDevice(g->o.device));
+    CK(cudaGetDevice(&g->device));
+    CK(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
+    CK(cudaMallocHost(&g->h_res, sizeof(PcgResult)));
+    CK(cudaMallocHost(&g->h_diff, sizeof(double)));
+    return GSLAM_OK;
+}
+
+static int finish_setup(gslam_graph *g, const std::vector<unsigned> &t1,
+                        const std::vector<unsigned> &t2) {
+    int rc = gslam_build_structure(g->n_poses, (int64_t)t1.size(), t1.data(), t2.data(),
+                                   g->o.sell_window, &g->S);
+    if (rc != GSLAM_OK) { g_last_error = "bad edge list"; return rc; }
+    rc = gslam_layout_upload(&g->L, g->S, g->st, g->device, g->o);
+    if (rc != GSLAM_OK) return rc;
+    DevMem &m = g->mem;
+    CK(dupload(m, g->st, &g->d_ctr_ptr, g->S.ctr_ptr));
+    CK(dupload(m, g->st, &g->d_ctr, g->S.ctr));
+    CK(dupload(m, g->st, &g->d_xi_ptr, g->S.xi_ptr));
+    CK(dupload(m, g->st, &g->d_xi_ctr, g->S.xi_ctr));
+    CK(dalloc(m, &g->d_blocks, 42 * (size_t)g->n_edges));
+    CK(dalloc(m, &g->d_dx, 3 * (size_t)g->n_poses));
+    CK(cudaMemsetAsync(g->d_dx, 0, 3 * (size_t)g->n_poses * sizeof(double), g->st));
+    g->n_upd_blocks = std::max(1, std::min(4 * g->L.n_sm, (g->n_poses + 255) / 256));
+    CK(dalloc(m, &g->d_block_sums, (size_t)g->n_upd_blocks));
+    CK(dalloc(m, &g->d_diff, 1));
+    CK(cudaStreamSynchronize(g->st));
+    return GSLAM_OK;
+}
+
+int gslam_create_reference(const gslam_reference_graph *in, const gslam_opts *opts,
+                           gslam_graph **out) {
+    if (!in || !out) BAD("null argument");
+    *out = nullptr;
+    if (in->n_poses == 0 || !in->poses || !in->controls) BAD("n_poses == 0 or missing arrays");
+    if (in->n_poses > 0x3fffffffu) { g_last_error = "too many poses"; return GSLAM_ERR_TOO_LARGE; }
+    if (in->n_obs && (!in->obs_step || !in->obs_landmark || !in->obs)) BAD("missing observation arrays");
+    for (uint32_t i = 0; i < in->n_obs; i++)
+        if (in->obs_step[i] >= in->n_poses) BAD("observation step out of range");
+    gslam_graph *g = new gslam_graph();
+    int rc = common_setup(g, opts);
+    if (rc != GSLAM_OK) { gslam_destroy(g); return rc; }
+    g->factors = GSLAM_FACTORS_REFERENCE;
+    g->n_poses = (int)in->n_poses;
+    g->delta = in->delta;
+    g->lambda = in->lambda;
+    static const double def_mns[4] = { 0.19, 0.001, 0.13, 0.2 };
+    memcpy(g->mns, in->mns ? in->mns : def_mns, sizeof g->mns);
+    g->anchor = 1000000.0;
+    std::vector<unsigned> pj, pk;
+    gslam_obs_pairs(in->n_obs, in->obs_landmark, &pj, &pk);
+    g->n_obs_edges = (int64_t)pj.size();
+    g->n_edges = g->n_obs_edges + (g->n_poses - 1);
+    std::vector<unsigned> t1(g->n_edges), t2(g->n_edges);
+    for (int64_t e = 0; e < g->n_obs_edges; e++) {
+        t1[e] = in->obs_step[pj[e]];
+        t2[e] = in->obs_step[pk[e]];
+    }
+    for (int i = 0; i + 1 < g->n_poses; i++) {
+        t1[g->n_obs_edges + i] = (unsigned)i;
+        t2[g->n_obs_edges + i] = (unsigned)(i + 1);
+    }
+    DevMem &m = g->mem;
+    auto fail = [&](int code) { gslam_destroy(g); return code; };
+    if (dalloc(m, &g->d_poses, 3 * (size_t)g->n_poses) != cudaSuccess ||
+        dalloc(m, &g->d_controls, 2 * (size_t)g->n_poses) != cudaSuccess) {
+        g_last_error = "cudaMalloc failed";
+        return fail(GSLAM_ERR_CUDA);
+    }
+    cudaMemcpyAsync(g->d_poses, in->poses, 3 * (size_t)g->n_poses * sizeof(double),
+                    cudaMemcpyHostToDevice, g->st);
+    cudaMemcpyAsync(g->d_controls, in->controls, 2 * (size_t)g->n_poses * sizeof(double),
+                    cudaMemcpyHostToDevice, g->st);
+    std::vector<unsigned> zs(in->obs_step, in->obs_step + in->n_obs);
+    std::vector<double> zrb(in->obs, in->obs + 2 * (size_t)in->n_obs);
+    if (dupload(m, g->st, &g->d_z_step, zs) != cudaSuccess ||
+        dupload(m, g->st, &g->d_z_rb, zrb) != cudaSuccess ||
+        dupload(m, g->st, &g->d_pj, pj) != cudaSuccess ||
+        dupload(m, g->st, &g->d_pk, pk) != cudaSuccess) {
+        g_last_error = "upload failed";
+        return fail(GSLAM_ERR_CUDA);
+    }
+    rc = finish_setup(g, t1, t2);
+    if (rc != GSLAM_OK) return fail(rc);
+    *out = g;
+    return GSLAM_OK;
+}
+
+int gslam_create_se2(const gslam_se2_graph *in, const gslam_opts *opts, gslam_graph **out) {
+    if (!in || !out) BAD("null argument");
+    *out = nullptr;
+    if (in->n_poses == 0 || !in->poses) BAD("n_poses == 0 or missing poses");
+    if (in->n_edges && (!in->edge_i || !in->edge_j || !in->meas || !in->log_w)) BAD("missing edge arrays");
+    for (uint32_t e = 0; e < in->n_edges; e++)
+        if (in->edge_i[e] >= in->n_poses || in->edge_j[e] >= in->n_poses) BAD("edge pose out of range");
+    gslam_graph *g = new gslam_graph();
+    int rc = common_setup(g, opts);
+    if (rc != GSLAM_OK) { gslam_destroy(g); return rc; }
+    g->factors = GSLAM_FACTORS_SE2;
+    g->n_poses = (int)in->n_poses;
+    g->lambda = in->lambda;
+    g->anchor = in->anchor;
+    g->n_obs_edges = 0;
+    g->n_edges = in->n_edges;
+    std::vector<unsigned> t1(in->edge_i, in->edge_i + in->n_edges), t2(in->edge_j, in->edge_j + in->n_edges);
+    std::vector<double> meas(in->meas, in->meas + 3 * (size_t)in->n_edges);
+    /* information weights exp(log_w), computed once here; lambda multiplies on device */
+    std::vector<double> lw(3 * (size_t)in->n_edges);
+    for (size_t k = 0; k < lw.size(); k++) lw[k] = std::exp(in->log_w[k]);
+    DevMem &m = g->mem;
+    auto fail = [&](int code) { gslam_destroy(g); return code; };
+    if (dalloc(m, &g->d_poses, 3 * (size_t)g->n_poses) != cudaSuccess ||
+        dupload(m, g->st, &g->d_ei, t1) != cudaSuccess || dupload(m, g->st, &g->d_ej, t2) != cudaSuccess ||
+        dupload(m, g->st, &g->d_meas, meas) != cudaSuccess || dupload(m, g->st, &g->d_info, lw) != cudaSuccess) {
+        g_last_error = "upload failed";
+        return fail(GSLAM_ERR_CUDA);
+    }
+    cudaMemcpyAsync(g->d_poses, in->poses, 3 * (size_t)g->n_poses * sizeof(double),
+                    cudaMemcpyHostToDevice, g->st);
+    rc = finish_setup(g, t1, t2);
+    if (rc != GSLAM_OK) return fail(rc);
+    *out = g;
+    return GSLAM_OK;
+}
+
+int gslam_destroy(gslam_graph *g) {
+    if (!g) return GSLAM_OK;
+    if (g->st) cudaStreamSynchronize(g->st);
+    gslam_layout_release(&g->L);
+    g->mem.release();
+    if (g->h_res) cudaFreeHost(g->h_res);
+    if (g->h_diff) cudaFreeHost(g->h_diff);
+    if (g->st) cudaStreamDestroy(g->st);
+    delete g;
+    return GSLAM_OK;
+}
+
+int gslam_set_opts(gslam_graph *g, const gslam_opts *opts) {
+    if (!g || !opts) BAD("null argument");
+    const int window = g->o.sell_window;
+    const int threads = g->o.threads_per_cta, cps = g->o.ctas_per_sm;
+    g->o = *opts;
+    g->o.sell_window = window; /* the layout is fixed at creation */
+    if ((opts->threads_per_cta && opts->threads_per_cta != threads) ||
+        (opts->ctas_per_sm && opts->ctas_per_sm != cps)) {
+        int block = opts->threads_per_cta ? opts->threads_per_cta : g->L.block;
+        int maxg = pcg_max_grid(g->o.precision, block, g->device);
+        if (maxg <= 0) { g_last_error = "unsupported block size"; return GSLAM_ERR_BAD_INPUT; }
+        int c = opts->ctas_per_sm ? opts->ctas_per_sm : 1;
+        int warps = block / 32;
+        int needed = (g->L.n_slices + warps - 1) / warps;
+        int grid = std::max(1, std::min(std::min(maxg, c * g->L.n_sm), needed));
+        if (grid > g->L.max_grid_alloc()) { g_last_error = "grid exceeds allocation"; return GSLAM_ERR_BAD_INPUT; }
+        g->L.block = block;
+        g->L.grid = grid;
+    }
+    g->o.threads_per_cta = g->L.block;
+    return GSLAM_OK;
+}
+
+int gslam_sizes(const gslam_graph *g, int64_t *n_poses, int64_t *n_edges, int64_t *nnzb,
+                int64_t *nnz) {
+    if (!g) BAD("null handle");
+    if (n_poses) *n_poses = g->n_poses;
+    if (n_edges) *n_edges = g->n_edges;
+    if (nnzb) *nnzb = g->S.nnzb;
+    if (nnz) *nnz = (int64_t)g->S.csr_col.size();
+    return GSLAM_OK;
+}
+
+int gslam_set_poses(gslam_graph *g, const double *poses) {
+    if (!g || !poses) BAD("null argument");
+    CK(cudaMemcpyAsync(g->d_poses, poses, 3 * (size_t)g->n_poses * sizeof(double),
+                       cudaMemcpyHostToDevice, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    return GSLAM_OK;
+}
+
+int gslam_get_poses(gslam_graph *g, double *poses) {
+    if (!g || !poses) BAD("null argument");
+    CK(cudaMemcpyAsync(poses, g->d_poses, 3 * (size_t)g->n_poses * sizeof(double),
+                       cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    return GSLAM_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* stages                                                                    */
+/* ------------------------------------------------------------------------ */
+
+int gslam_linearise(gslam_graph *g) {
+    if (!g) BAD("null handle");
+    if (g->factors == GSLAM_FACTORS_REFERENCE) {
+        launch_obs_edges(g->st, g->n_obs_edges, g->d_pj, g->d_pk, g->d_z_step, g->d_z_rb,
+                         g->d_poses, g->d_blocks);
+        launch_motion_edges(g->st, g->n_poses, g->n_obs_edges, g->d_controls, g->delta, g->lambda,
+                            g->mns, g->d_poses, g->d_blocks);
+    } else {
+        launch_se2_edges(g->st, g->n_edges, 0, g->d_ei, g->d_ej, g->d_meas, g->d_info, g->lambda,
+                         g->d_poses, g->d_blocks);
+    }
+    CK(cudaGetLastError());
+    return GSLAM_OK;
+}
+
+int gslam_assemble_ex(gslam_graph *g, const double *blocks, double *csr_vals, double *xi_orig) {
+    float *v32 = nullptr;
+    if (g->o.precision == GSLAM_PREC_MIXED) {
+        int rc = gslam_layout_ensure_fp32(&g->L, g->st);
+        if (rc != GSLAM_OK) return rc;
+        v32 = g->L.val32;
+    }
+    launch_assemble(g->st, g->L.n_slots, g->d_ctr_ptr, g->d_ctr, blocks, g->S.anchor_slot, g->anchor,
+                    g->L.val, v32, g->L.slot_csr, g->L.chunk_slice, g->L.row_len, csr_vals);
+    launch_assemble_xi(g->st, g->n_poses, g->d_xi_ptr, g->d_xi_ctr, blocks, g->L.b4, g->L.perm,
+                       xi_orig);
+    CK(cudaGetLastError());
+    return GSLAM_OK;
+}
+
+int gslam_assemble(gslam_graph *g) {
+    if (!g) BAD("null handle");
+    return gslam_assemble_ex(g, g->d_blocks, nullptr, nullptr);
+}
+
+int gslam_assemble_from_edges(gslam_graph *g, const double *d_blocks) {
+    if (!g || !d_blocks) BAD("null argument");
+    return gslam_assemble_ex(g, d_blocks, nullptr, nullptr);
+}
+
+int gslam_solve(gslam_graph *g, gslam_solve_stats *stats) {
+    if (!g) BAD("null handle");
+    int rc = gslam_layout_solve(&g->L, g->st, g->o, g->h_res, stats);
+    g->last_res = *g->h_res;
+    return rc;
+}
+
+int gslam_update(gslam_graph *g, double *diff) {
+    if (!g) BAD("null handle");
+    launch_pose_update(g->st, g->n_poses, g->L.iperm, g->L.x4, g->d_poses, g->d_dx, g->o.angle_wrap,
+                       g->d_block_sums, g->n_upd_blocks, g->d_diff);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(g->h_diff, g->d_diff, sizeof(double), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    if (diff) *diff = *g->h_diff;
+    return GSLAM_OK;
+}
+
+int gslam_round(gslam_graph *g, gslam_solve_stats *stats) {
+    if (!g) BAD("null handle");
+    int rc = gslam_linearise(g);
+    if (rc != GSLAM_OK) return rc;
+    rc = gslam_assemble(g);
+    if (rc != GSLAM_OK) return rc;
+    gslam_solve_stats st;
+    rc = gslam_solve(g, &st);
+    if (rc != GSLAM_OK) { if (stats) *stats = st; return rc; }
+    double diff = 0.0;
+    rc = gslam_update(g, &diff);
+    st.diff = diff;
+    if (stats) *stats = st;
+    return rc;
+}
+
+int gslam_run(gslam_graph *g, int max_rounds, double *diffs, int *rounds_done) {
+    if (!g) BAD("null handle");
+    double best = 1e30;
+    int no_improve = 0, n = 0;
+    for (int r = 1; r <= max_rounds; r++) {
+        gslam_solve_stats st;
+        int rc = gslam_round(g, &st);
+        if (rc != GSLAM_OK) { if (rounds_done) *rounds_done = n; return rc; }
+        n = r;
+        if (diffs) diffs[r - 1] = st.diff;
+        if (st.diff < 0.01) break;                   /* GSLAM.c:120 */
+        if (st.diff < best) { best = st.diff; no_improve = 0; }
+        else if (++no_improve >= 20) break;          /* GSLAM.c:124-129 */
+    }
+    if (rounds_done) *rounds_done = n;
+    return GSLAM_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* read-back helpers                                                         */
+/* ------------------------------------------------------------------------ */
+
+int gslam_get_edge_blocks(gslam_graph *g, double *blocks) {
+    if (!g || !blocks) BAD("null argument");
+    CK(cudaMemcpyAsync(blocks, g->d_blocks, 42 * (size_t)g->n_edges * sizeof(double),
+                       cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    return GSLAM_OK;
+}
+
+int gslam_get_csr(gslam_graph *g, int *row_ptr, int *col_idx, double *values, double *xi) {
+    if (!g) BAD("null handle");
+    const size_t nnz = g->S.csr_col.size(), dim = 3 * (size_t)g->n_poses;
+    if (row_ptr) memcpy(row_ptr, g->S.csr_row_ptr.data(), (dim + 1) * sizeof(int));
+    if (col_idx) memcpy(col_idx, g->S.csr_col.data(), nnz * sizeof(int));
+    if (values || xi) {
+        if (!g->d_csr_tmp) {
+            CK(dalloc(g->mem, &g->d_csr_tmp, nnz));
+            CK(dalloc(g->mem, &g->d_xi_tmp, dim));
+        }
+        launch_sell_to_csr(g->st, g->L.n_slots, g->L.slot_csr, g->L.chunk_slice, g->L.row_len,
+                           g->L.val, g->d_csr_tmp);
+        launch_scatter_vec(g->st, g->n_poses, g->L.perm, g->L.b4, g->d_xi_tmp);
+        CK(cudaGetLastError());
+        if (values) CK(cudaMemcpyAsync(values, g->d_csr_tmp, nnz * sizeof(double), cudaMemcpyDeviceToHost, g->st));
+        if (xi) CK(cudaMemcpyAsync(xi, g->d_xi_tmp, dim * sizeof(double), cudaMemcpyDeviceToHost, g->st));
+        CK(cudaStreamSynchronize(g->st));
+    }
+    return GSLAM_OK;
+}
+
+int gslam_get_dx(gslam_graph *g, double *dx) {
+    if (!g || !dx) BAD("null argument");
+    double *tmp = nullptr;
+    if (!g->d_xi_tmp) CK(dalloc(g->mem, &g->d_xi_tmp, 3 * (size_t)g->n_poses));
+    tmp = g->d_xi_tmp;
+    launch_scatter_vec(g->st, g->n_poses, g->L.perm, g->L.x4, tmp);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dx, tmp, 3 * (size_t)g->n_poses * sizeof(double), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    return GSLAM_OK;
+}
+
+int gslam_get_diag_inv(gslam_graph *g, double *dinv) {
+    if (!g || !dinv) BAD("null argument");
+    const size_t n = 9 * 32 * (size_t)g->L.n_slices;
+    std::vector<double> h(n);
+    CK(cudaMemcpyAsync(h.data(), g->L.dinv, n * sizeof(double), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    for (int old = 0; old < g->n_poses; old++) {
+        const int nr = g->S.iperm[old];
+        for (int e = 0; e < 9; e++) dinv[9 * (size_t)old + e] = h[288 * (size_t)(nr >> 5) + 32 * e + (nr & 31)];
+    }
+    return GSLAM_OK;
+}
+
+int gslam_spmv(gslam_graph *g, const double *d_x, double *d_y) {
+    if (!g || !d_x || !d_y) BAD("null argument");
+    launch_gather_vec(g->st, g->n_poses, g->L.perm, d_x, g->L.p4a);
+    launch_spmv64(g->st, g->n_poses, g->L.n_slices, g->L.slice_ptr, g->L.row_len, g->L.col, g->L.val,
+                  g->L.p4a, g->L.q4);
+    launch_scatter_vec(g->st, g->n_poses, g->L.perm, g->L.q4, d_y);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(g->st));
+    return GSLAM_OK;
+}
+
+int gslam_spmv_bench(gslam_graph *g, int prec, int reps, float *ms) {
+    if (!g || !ms || reps <= 0) BAD("bad argument");
+    if (prec == 1) {
+        int rc = gslam_layout_ensure_fp32(&g->L, g->st);
+        if (rc != GSLAM_OK) return rc;
+    }
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, g->st));
+    for (int i = 0; i < reps; i++) {
+        if (prec == 1)
+            launch_spmv32(g->st, g->n_poses, g->L.n_slices, g->L.slice_ptr, g->L.row_len, g->L.col,
+                          g->L.val32, g->L.f[3], g->L.f[5]);
+        else
+            launch_spmv64(g->st, g->n_poses, g->L.n_slices, g->L.slice_ptr, g->L.row_len, g->L.col,
+                          g->L.val, g->L.p4a, g->L.q4);
+    }
+    CK(cudaEventRecord(b, g->st));
+    CK(cudaEventSynchronize(b));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = t / reps;
+    return GSLAM_OK;
+}

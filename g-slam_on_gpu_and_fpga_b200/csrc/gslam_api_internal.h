@@ -1,0 +1,83 @@
+/* gslam_api_internal.h — device-side objects behind the C ABI (internal). */
+#ifndef GSLAM_API_INTERNAL_H
+#define GSLAM_API_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gslam.h"
+#include "gslam_internal.h"
+#include "kernels.cuh"
+
+/* Device allocations owned by one object, released together. */
+struct DevMem {
+    std::vector<void *> ptrs;
+    void release();
+};
+
+/* Device copy of a layout plus the solver's work vectors. */
+struct DevLayout {
+    DevMem mem;
+    int n_rows = 0, n_slices = 0;
+    int64_t n_slots = 0;
+    int *perm = nullptr, *iperm = nullptr, *row_len = nullptr, *col = nullptr;
+    int *diag_slot = nullptr, *chunk_slice = nullptr;
+    int64_t *slice_ptr = nullptr, *slot_csr = nullptr;
+    double *val = nullptr, *dinv = nullptr;
+    float *val32 = nullptr;
+    double *b4 = nullptr, *x4 = nullptr, *r4 = nullptr, *z4 = nullptr;
+    double *p4a = nullptr, *p4b = nullptr, *q4 = nullptr;
+    float *f[6] = { nullptr, nullptr, nullptr, nullptr, nullptr, nullptr };
+    double *partials = nullptr;
+    GridSync *gs = nullptr;
+    PcgResult *res = nullptr;
+    int grid = 0, block = 0, n_sm = 0;
+    int partial_capacity = 0;
+    int max_grid_alloc() const { return partial_capacity; }
+};
+
+struct gslam_graph {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    gslam_opts o;
+    int factors = GSLAM_FACTORS_REFERENCE;
+    gslam_structure S;
+    DevLayout L;
+    DevMem mem;
+    int n_poses = 0;
+    int64_t n_obs_edges = 0, n_edges = 0;
+    double delta = 1.0, lambda = 1.0, mns[4] = { 0.19, 0.001, 0.13, 0.2 };
+    double anchor = 1000000.0;
+    /* reference factor inputs */
+    double *d_poses = nullptr, *d_controls = nullptr, *d_z_rb = nullptr;
+    unsigned *d_z_step = nullptr, *d_pj = nullptr, *d_pk = nullptr;
+    /* SE(2) factor inputs */
+    unsigned *d_ei = nullptr, *d_ej = nullptr;
+    double *d_meas = nullptr, *d_info = nullptr; /* info = exp(log_w) */
+    /* per-round buffers */
+    double *d_blocks = nullptr;
+    int64_t *d_ctr_ptr = nullptr, *d_ctr = nullptr, *d_xi_ptr = nullptr, *d_xi_ctr = nullptr;
+    double *d_dx = nullptr, *d_block_sums = nullptr, *d_diff = nullptr;
+    int n_upd_blocks = 1;
+    double *d_csr_tmp = nullptr, *d_xi_tmp = nullptr;
+    PcgResult *h_res = nullptr;
+    double *h_diff = nullptr;
+    PcgResult last_res = {};
+};
+
+int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st, int device,
+                        const gslam_opts &o);
+int gslam_layout_ensure_fp32(DevLayout *L, cudaStream_t st);
+int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgResult *h_res,
+                       gslam_solve_stats *stats);
+void gslam_layout_release(DevLayout *L);
+/* Assembles Omega / xi from edge blocks; optionally also writes the reference's CSR
+ * values (csr_vals) and xi in original order (xi_orig), both device pointers. */
+int gslam_assemble_ex(gslam_graph *g, const double *blocks, double *csr_vals, double *xi_orig);
+/* Records an error message for gslam_last_error(). */
+void gslam_set_last_error(const char *msg);
+void gslam_set_error(const char *fmt, const char *what, int code);
+
+#endif

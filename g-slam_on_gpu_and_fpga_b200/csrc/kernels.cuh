@@ -1,0 +1,92 @@
+/* kernels.cuh — launchers of libgslam's device kernels (internal). */
+#ifndef GSLAM_KERNELS_CUH
+#define GSLAM_KERNELS_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+void launch_obs_edges(cudaStream_t st, int64_t n, const unsigned *pj, const unsigned *pk,
+                      const unsigned *z_step, const double *z_rb, const double *poses,
+                      double *blocks);
+void launch_motion_edges(cudaStream_t st, int n_poses, int64_t first_edge, const double *controls,
+                         double delta, double lambda, const double *mns, const double *poses,
+                         double *blocks);
+void launch_se2_edges(cudaStream_t st, int64_t n, int64_t first_edge, const unsigned *ei,
+                      const unsigned *ej, const double *meas, const double *info, double lambda,
+                      const double *poses, double *blocks);
+void launch_assemble(cudaStream_t st, int64_t n_slots, const int64_t *ctr_ptr, const int64_t *ctr,
+                     const double *blocks, int64_t anchor_slot, double anchor, double *val,
+                     float *val32, const int64_t *slot_csr, const int *chunk_slice,
+                     const int *row_len, double *csr_vals);
+void launch_sell_to_csr(cudaStream_t st, int64_t n_slots, const int64_t *slot_csr,
+                        const int *chunk_slice, const int *row_len, const double *val,
+                        double *csr_vals);
+void launch_assemble_xi(cudaStream_t st, int n_rows, const int64_t *xi_ptr, const int64_t *xi_ctr,
+                        const double *blocks, double *b4, const int *perm, double *xi_orig);
+void launch_csr_to_sell(cudaStream_t st, int64_t n_slots, const int64_t *slot_csr,
+                        const int *chunk_slice, const int *row_len, const double *csr_vals,
+                        double *val, float *val32);
+void launch_gather_vec(cudaStream_t st, int n_rows, const int *perm, const double *src, double *dst4);
+void launch_scatter_vec(cudaStream_t st, int n_rows, const int *perm, const double *src4, double *dst);
+void launch_diag_inv(cudaStream_t st, int n_rows, const int *diag_slot, const double *val,
+                     double *dinv);
+void launch_pose_update(cudaStream_t st, int n_rows, const int *iperm, const double *x4,
+                        double *poses, double *dx, int wrap, double *block_sums, int n_blocks,
+                        double *diff_out);
+
+/* ---- solver ---- */
+
+struct GridSync {
+    unsigned count;
+    unsigned gen;
+    int abort;
+    int pad;
+};
+
+struct PcgResult {
+    int iterations;
+    int reason;
+    int refinements;
+    int timeout;
+    double rnorm;
+    double bnorm;
+};
+
+struct PcgParams {
+    int n_rows;
+    int n_slices;
+    const int64_t *slice_ptr;
+    const int *row_len;
+    const int *col;
+    const double *val;     /* FP64 values (slot layout) */
+    const float *val32;    /* FP32 copy (mixed) */
+    const double *dinv;    /* block-Jacobi inverses (slot layout) */
+    const double *b4;      /* right-hand side, padded new order */
+    double *x4, *r4, *z4, *p4a, *p4b, *q4;  /* FP64 work vectors */
+    float *xf4, *rf4, *zf4, *pfa4, *pfb4, *qf4; /* FP32 work vectors (mixed) */
+    double tol_rel;
+    int max_iter;
+    double inner_tol;
+    int inner_max_iter;
+    int max_refine;
+    double *partials;      /* [2][4 * gridDim.x]: two alternating buffers */
+    GridSync *gs;
+    PcgResult *res;
+    long long spin_limit;  /* clock cycles a barrier may wait */
+    int absent_cta;        /* test hook: CTA that leaves before its first barrier, -1 = none */
+};
+
+/* Cooperative launch of the persistent solver; returns the CUDA error. */
+cudaError_t launch_pcg(cudaStream_t st, const PcgParams &p, int precision, int grid, int block);
+/* Largest co-resident grid for the solver at this block size (0 if unsupported). */
+int pcg_max_grid(int precision, int block, int device);
+
+/* Standalone SpMV y = A x on padded new-order vectors (FP64 or FP32 values). */
+void launch_spmv64(cudaStream_t st, int n_rows, int n_slices, const int64_t *slice_ptr,
+                   const int *row_len, const int *col, const double *val, const double *x4,
+                   double *y4);
+void launch_spmv32(cudaStream_t st, int n_rows, int n_slices, const int64_t *slice_ptr,
+                   const int *row_len, const int *col, const float *val, const float *x4,
+                   float *y4);
+
+#endif

@@ -1,0 +1,195 @@
+/*
+ * gslam.h — C ABI of libgslam, a B200 (sm_100a) Graph-SLAM back-end.
+ *
+ * One handle = one pose graph resident on one GPU. Every call returns an int
+ * status (GSLAM_OK or a negative GSLAM_ERR_*); arguments are plain pointers and
+ * sizes. Pointers named d_* are device pointers on the handle's GPU; all others
+ * are host pointers. Calls on one handle must not overlap; different handles are
+ * independent (each owns its stream and buffers).
+ *
+ * The reference (isaacyhe/G-SLAM_on_GPU_and_FPGA) has no handle API: its path is
+ * the program in src/cpu_pcg_fp64 (GSLAM.c main, one process = one graph) and
+ * the static-state GPU twin src/gpu_pcg_fp64/device_graph.cuh:23-91. The entry
+ * points below replace that path; gslam_dropin.h carries the reference's own
+ * signatures on top of them.
+ */
+#ifndef GSLAM_H
+#define GSLAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference only ever exit(1)s: device_graph.cu:99-106) ---- */
+#define GSLAM_OK 0
+#define GSLAM_ERR_BAD_INPUT -1      /* sizes, indices or values out of range */
+#define GSLAM_ERR_CUDA -2           /* a CUDA runtime call failed */
+#define GSLAM_ERR_DEVICE_TIMEOUT -3 /* a bounded device wait gave up (kernel returned) */
+#define GSLAM_ERR_NOT_CONVERGED -4  /* solver stopped at max_iter above tolerance (informational) */
+#define GSLAM_ERR_TOO_LARGE -5      /* exceeds a fixed capacity (32-bit CSR, scratch size) */
+#define GSLAM_ERR_NO_DEVICE -6      /* no sm_100 device / cooperative launch unavailable */
+
+/* ---- solver precision ---- */
+#define GSLAM_PREC_FP64 0  /* FP64 block-Jacobi PCG (the reference's arithmetic) */
+#define GSLAM_PREC_MIXED 1 /* FP32 SpMV / vectors inside FP64 iterative refinement */
+
+/* ---- factor families ---- */
+#define GSLAM_FACTORS_REFERENCE 0 /* ObsEdge + MotionEdge of src/cpu_pcg_fp64 */
+#define GSLAM_FACTORS_SE2 1       /* SE(2) between-factors with diagonal information */
+
+/* PCG termination reasons (gslam_solve_stats.reason) */
+#define GSLAM_STOP_TOL 0     /* ||r|| < tol * ||b|| */
+#define GSLAM_STOP_MAXIT 1   /* iteration cap reached */
+#define GSLAM_STOP_PQ_ZERO 2 /* p.Ap == 0 (MatrixOps.c:357) */
+#define GSLAM_STOP_TIMEOUT 3 /* device barrier wait gave up */
+
+typedef struct gslam_opts {
+    int precision;        /* GSLAM_PREC_*; default FP64 */
+    double tol;           /* relative residual tolerance; reference 1e-6 (MatrixOps.c:345) */
+    int max_iter;         /* PCG iteration cap; reference 500 (MatrixOps.c:347) */
+    int sell_window;      /* rows sorted by block count inside windows of this size; 0 = auto */
+    int threads_per_cta;  /* persistent PCG block size; 0 = auto */
+    int ctas_per_sm;      /* persistent PCG CTAs per SM; 0 = auto (occupancy) */
+    int angle_wrap;       /* wrap theta to (-pi, pi] in the pose update; 0 for the reference */
+    double inner_tol;     /* mixed: inner FP32 relative tolerance per refinement step */
+    int inner_max_iter;   /* mixed: inner iteration cap per refinement step */
+    int max_refine;       /* mixed: outer refinement steps cap */
+    int device;           /* CUDA device ordinal; -1 = current */
+    double barrier_timeout_ms; /* a solver barrier gives up after this long; 0 = 2000 ms */
+    int test_absent_cta;  /* test hook: this solver CTA never arrives at its first barrier, so
+                             the others time out (checks the bounded wait); -1 = off */
+} gslam_opts;
+
+typedef struct gslam_solve_stats {
+    int iterations;       /* PCG iterations (mixed: total inner iterations) */
+    int refinements;      /* mixed: outer FP64 steps; FP64: 0 */
+    int reason;           /* GSLAM_STOP_* */
+    double rel_residual;  /* ||b - A x|| / ||b|| as tracked by the solver */
+    double diff;          /* ||dx|| / sqrt(dim) (GSLAM.c:104-105) */
+} gslam_solve_stats;
+
+/* Inputs of the reference's factor family, as read_data produces them (GSLAM.c:415-493). */
+typedef struct gslam_reference_graph {
+    uint32_t n_poses;          /* size_of_hat_xs; dim = 3 * n_poses */
+    const double *poses;       /* [3 * n_poses] x, y, theta (initial guess) */
+    const double *controls;    /* [2 * n_poses] nu, omega of each step (row 0 unused) */
+    double delta;              /* time step */
+    double lambda;             /* motion-edge weight (argv[2]) */
+    const double *mns;         /* [4] motion noise; NULL = {0.19, 0.001, 0.13, 0.2} */
+    uint32_t n_obs;            /* observations */
+    const uint32_t *obs_step;  /* [n_obs] pose index of each observation */
+    const uint32_t *obs_landmark; /* [n_obs] landmark id */
+    const double *obs;         /* [2 * n_obs] range, bearing */
+} gslam_reference_graph;
+
+/* SE(2) pose graph: edge e constrains pose j relative to pose i. */
+typedef struct gslam_se2_graph {
+    uint32_t n_poses;
+    const double *poses;       /* [3 * n_poses] initial guess */
+    uint32_t n_edges;
+    const uint32_t *edge_i;    /* [n_edges] */
+    const uint32_t *edge_j;    /* [n_edges] */
+    const double *meas;        /* [3 * n_edges] dx, dy, dtheta in the frame of pose i */
+    const double *log_w;       /* [3 * n_edges] log information weights (log 1/sigma^2) */
+    double lambda;             /* global information scale */
+    double anchor;             /* prior weight on pose 0 (1e6 like the reference) */
+} gslam_se2_graph;
+
+typedef struct gslam_graph gslam_graph;
+
+/* Fills the defaults: FP64, tol 1e-6, max_iter 500, reference behaviour. */
+int gslam_opts_default(gslam_opts *opts);
+
+/* Builds a resident graph of the reference factor family. */
+int gslam_create_reference(const gslam_reference_graph *in, const gslam_opts *opts,
+                           gslam_graph **out);
+/* Builds a resident SE(2) pose graph (odometry + loop closures). */
+int gslam_create_se2(const gslam_se2_graph *in, const gslam_opts *opts, gslam_graph **out);
+int gslam_destroy(gslam_graph *g);
+
+/* Replaces solver options (precision, tolerances) of an existing graph. */
+int gslam_set_opts(gslam_graph *g, const gslam_opts *opts);
+/* Sizes: n_poses, n_edges (all factors), nnzb (3x3 blocks), nnz (scalar CSR). */
+int gslam_sizes(const gslam_graph *g, int64_t *n_poses, int64_t *n_edges, int64_t *nnzb,
+                int64_t *nnz);
+
+/* Pose state (x, y, theta per pose, original order). */
+int gslam_set_poses(gslam_graph *g, const double *poses);
+int gslam_get_poses(gslam_graph *g, double *poses);
+
+/*
+ * One Gauss-Newton round on the device: linearise every edge, assemble Omega and
+ * xi, invert the 3x3 diagonal blocks, solve Omega dx = xi, add dx to the poses.
+ * stats may be NULL. Equivalent to one iteration of GSLAM.c:55-139.
+ */
+int gslam_round(gslam_graph *g, gslam_solve_stats *stats);
+
+/*
+ * Up to max_rounds rounds with the reference's stop rules (diff < 0.01, or 20
+ * rounds without a new best diff). diffs[max_rounds] (may be NULL) receives the
+ * per-round diff; *rounds_done the number executed.
+ */
+int gslam_run(gslam_graph *g, int max_rounds, double *diffs, int *rounds_done);
+
+/* ---- stages, for callers that drive the round themselves ---- */
+int gslam_linearise(gslam_graph *g);                 /* edge blocks from current poses */
+int gslam_assemble(gslam_graph *g);                  /* Omega, xi, block-Jacobi inverse */
+int gslam_solve(gslam_graph *g, gslam_solve_stats *stats); /* dx = Omega^-1 xi */
+int gslam_update(gslam_graph *g, double *diff);      /* poses += dx */
+
+/* Edge blocks in the reference's Edge order: [n_edges][42] = UL, UR, BL, BR, xi_u, xi_b. */
+int gslam_get_edge_blocks(gslam_graph *g, double *blocks);
+/* Assembles from caller-provided device edge blocks (same layout) instead of linearising. */
+int gslam_assemble_from_edges(gslam_graph *g, const double *d_blocks);
+/* Omega and xi in the reference's scalar CSR (MatrixOps.h:21-27): row_ptr[3N+1], col_idx[nnz],
+ * values[nnz], xi[3N]; any pointer may be NULL. */
+int gslam_get_csr(gslam_graph *g, int *row_ptr, int *col_idx, double *values, double *xi);
+/* The last solution dx[3N] (original order). */
+int gslam_get_dx(gslam_graph *g, double *dx);
+/* Block-Jacobi inverses [N][9] (original order). */
+int gslam_get_diag_inv(gslam_graph *g, double *dinv);
+
+/* y = Omega x on device pointers in original order [3N] (FP64, row sums in column order). */
+int gslam_spmv(gslam_graph *g, const double *d_x, double *d_y);
+/* Runs `reps` FP64 (prec 0) or FP32 (prec 1) SpMVs on the resident matrix; *ms = mean ms each. */
+int gslam_spmv_bench(gslam_graph *g, int prec, int reps, float *ms);
+
+/* ---- host-only utilities (no GPU needed) ---- */
+/* Observation-edge order of make_edges (src/cpu_pcg_fp64/GSLAM.c:222-318): pairs of z-list
+ * indices (pj[e], pk[e]). Call with cap 0 to get the count in *n_pairs. */
+int gslam_obs_edge_order(uint32_t n_obs, const uint32_t *obs_landmark, uint32_t *pj, uint32_t *pk,
+                         int64_t cap, int64_t *n_pairs);
+/* The reference's scalar CSR pattern (MatrixOps.c:175-221) for edges (t1[e], t2[e]) between
+ * n_poses poses plus the anchor on pose 0. Call with col_idx NULL to get *nnz. */
+int gslam_csr_pattern(uint32_t n_poses, int64_t n_edges, const uint32_t *t1, const uint32_t *t2,
+                      int *row_ptr, int *col_idx, int64_t *nnz);
+
+/* ---- reference log files (src/cpu_pcg_fp64/GSLAM.c:415-493, data/README.md) ---- */
+typedef struct gslam_log {
+    double delta;
+    uint32_t n_u, n_x, n_z;
+    uint32_t *u_step;   /* [n_u] */
+    double *u;          /* [2 * n_u] nu, omega */
+    uint32_t *x_step;   /* [n_x] */
+    double *x;          /* [3 * n_x] x, y, theta */
+    uint32_t *z_step;   /* [n_z] */
+    uint32_t *z_lm;     /* [n_z] */
+    double *z;          /* [2 * n_z] range, bearing */
+} gslam_log;
+/* Parses a log like read_data: space-separated tokens; `u`, `x`, `z` records; any
+ * other first token sets delta from the second. Returns GSLAM_ERR_BAD_INPUT for a
+ * missing file or a truncated record. Free with gslam_free_log. */
+int gslam_read_log(const char *path, gslam_log **out);
+void gslam_free_log(gslam_log *log);
+
+/* Library version string and the error text of the last failing call on this thread. */
+const char *gslam_version(void);
+const char *gslam_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

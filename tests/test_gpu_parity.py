@@ -1,0 +1,349 @@
+"""GPU parity: libgslam's CUDA path against the C oracle, through the C ABI.
+
+Bit-exact: edge order, CSR pattern, edge blocks (vs the oracle's correctly
+rounded flavour), Omega and xi (also from the reference's own glibc edge
+blocks), block-Jacobi inverses, SpMV. Within stated tolerances: PCG solutions
+and multi-round poses (parallel dot products sum in a different order).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import assert_bitwise, load_pkg
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _cases():
+    G = load_pkg()
+    out = []
+    cg = G.synth.city_grid(64, seed=3, block=8)
+    out.append(("closures64", G.synth.to_reference_log(cg), 0.1))
+    cg = G.synth.city_grid(2000, seed=4, k_closures=6, radius=3.0)
+    out.append(("closures2000", G.synth.to_reference_log(cg), 1.0))
+    out.append(("landmarks600", G.synth.landmark_log(600, seed=7), 0.1))
+    out.append(("landmarks2500", G.synth.landmark_log(2500, seed=8), 1.0))
+    return out
+
+
+CASES = None
+
+
+def cases():
+    global CASES
+    if CASES is None:
+        CASES = _cases()
+    return CASES
+
+
+def _ograph(oracle, log):
+    return oracle.Graph(log.delta, log.u_step, log.u, log.x_step, log.x, log.z_step, log.z_lm, log.z)
+
+
+@pytest.fixture(scope="module", params=range(4), ids=["closures64", "closures2000", "landmarks600", "landmarks2500"])
+def case(request):
+    return cases()[request.param]
+
+
+def test_linearise_bitwise(case, oracle):
+    G = load_pkg()
+    name, log, lam = case
+    with G.PoseGraph.from_log(log, lam) as g:
+        g.linearise()
+        blocks = g.edge_blocks()
+    og = _ograph(oracle, log)
+    _, _, ob = oracle.linearise(og, og.x, lam, cr=True)
+    assert_bitwise(blocks, ob, f"{name} edge blocks")
+
+
+def test_assembly_bitwise(case, oracle):
+    G = load_pkg()
+    name, log, lam = case
+    og = _ograph(oracle, log)
+    t1, t2, ob = oracle.linearise(og, og.x, lam, cr=True)
+    rp, ci, va, xi = oracle.csr_build(og.dim, t1, t2, ob)
+    with G.PoseGraph.from_log(log, lam) as g:
+        g.linearise()
+        g.assemble()
+        grp, gci, gva, gxi = g.csr()
+    assert np.array_equal(grp, rp) and np.array_equal(gci, ci)
+    assert_bitwise(gva, va, f"{name} Omega")
+    assert_bitwise(gxi, xi, f"{name} xi")
+
+
+def test_assembly_of_reference_blocks_bitwise(case, oracle):
+    """Assembly fed the reference's own (glibc) edge blocks reproduces its Omega exactly."""
+    G = load_pkg()
+    name, log, lam = case
+    og = _ograph(oracle, log)
+    t1, t2, ob = oracle.linearise(og, og.x, lam, cr=False)
+    rp, ci, va, xi = oracle.csr_build(og.dim, t1, t2, ob)
+    d_blocks = torch.from_numpy(np.ascontiguousarray(ob)).cuda()
+    with G.PoseGraph.from_log(log, lam) as g:
+        g.assemble_from_edges(d_blocks.data_ptr())
+        _, _, gva, gxi = g.csr()
+    assert_bitwise(gva, va, f"{name} Omega from reference blocks")
+    assert_bitwise(gxi, xi, f"{name} xi from reference blocks")
+
+
+def test_diag_inv_and_spmv_bitwise(case, oracle):
+    G = load_pkg()
+    name, log, lam = case
+    og = _ograph(oracle, log)
+    t1, t2, ob = oracle.linearise(og, og.x, lam, cr=True)
+    rp, ci, va, xi = oracle.csr_build(og.dim, t1, t2, ob)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(og.dim)
+    with G.PoseGraph.from_log(log, lam) as g:
+        g.linearise()
+        g.assemble()
+        g.solve()
+        dinv = g.diag_inv()
+        d_x = torch.from_numpy(x).cuda()
+        d_y = torch.zeros_like(d_x)
+        g.spmv(d_x.data_ptr(), d_y.data_ptr())
+        torch.cuda.synchronize()
+        y = d_y.cpu().numpy()
+    assert_bitwise(dinv, oracle.diag_inv(rp, ci, va), f"{name} block-Jacobi inverses")
+    assert_bitwise(y, oracle.spmv(rp, ci, va, x), f"{name} SpMV")
+
+
+def test_pcg_solution_tolerance(case, oracle):
+    """Converged FP64 PCG (tol 1e-10): dx within 1e-7 relative of the oracle's."""
+    G = load_pkg()
+    name, log, lam = case
+    og = _ograph(oracle, log)
+    t1, t2, ob = oracle.linearise(og, og.x, lam, cr=True)
+    rp, ci, va, xi = oracle.csr_build(og.dim, t1, t2, ob)
+    x_ref, it_ref, _ = oracle.pcg(rp, ci, va, xi, tol=1e-10, max_iter=200000)
+    with G.PoseGraph.from_log(log, lam, tol=1e-10, max_iter=200000) as g:
+        g.linearise()
+        g.assemble()
+        st = g.solve()
+        dx = g.dx()
+    assert st.reason == G.abi.STOP_TOL
+    A = oracle.dense_from_csr(rp, ci, va) if og.dim <= 3000 else None
+    err = np.linalg.norm(dx - x_ref) / np.linalg.norm(x_ref)
+    assert err <= 1e-7, f"{name}: rel err {err:.3e} (iters {st.iterations} vs {it_ref})"
+    if A is not None:
+        res = np.linalg.norm(A @ dx - xi) / np.linalg.norm(xi)
+        assert res <= 1e-9
+    assert abs(st.iterations - it_ref) <= max(10, 0.05 * it_ref)
+
+
+def test_pcg_reference_settings(case, oracle):
+    """At the reference's settings (tol 1e-6, 500 iterations) the iteration count and
+    the solution agree closely with the reference PCG on the same Omega."""
+    G = load_pkg()
+    name, log, lam = case
+    og = _ograph(oracle, log)
+    t1, t2, ob = oracle.linearise(og, og.x, lam, cr=True)
+    rp, ci, va, xi = oracle.csr_build(og.dim, t1, t2, ob)
+    x_ref, it_ref, _ = oracle.pcg(rp, ci, va, xi)
+    with G.PoseGraph.from_log(log, lam) as g:
+        g.linearise()
+        g.assemble()
+        st = g.solve()
+        dx = g.dx()
+    err = np.linalg.norm(dx - x_ref) / np.linalg.norm(x_ref)
+    assert err <= 1e-3, f"{name}: rel err {err:.3e}"
+    assert abs(st.iterations - it_ref) <= max(3, 0.02 * it_ref)
+
+
+def test_rounds_match_oracle(case, oracle):
+    """Three GN rounds at tol 1e-10: poses within 1e-7 (relative to pose scale)."""
+    G = load_pkg()
+    name, log, lam = case
+    og = _ograph(oracle, log)
+    p_ref, diffs_ref, _ = oracle.run(og, lam, 3, cr=True, tol=1e-10, max_iter=200000)
+    with G.PoseGraph.from_log(log, lam, tol=1e-10, max_iter=200000) as g:
+        diffs = [g.round().diff for _ in range(len(diffs_ref))]
+        p = g.poses
+    scale = max(1.0, np.abs(p_ref).max())
+    assert np.abs(p - p_ref).max() <= 1e-7 * scale
+    assert np.allclose(diffs, diffs_ref, rtol=1e-6)
+
+
+def test_deterministic(oracle):
+    G = load_pkg()
+    _, log, lam = cases()[1]
+    outs = []
+    for _ in range(2):
+        with G.PoseGraph.from_log(log, lam) as g:
+            g.round()
+            g.round()
+            outs.append(g.poses)
+    assert_bitwise(outs[0], outs[1], "repeat run")
+
+
+def test_se2_blocks_bitwise(oracle):
+    G = load_pkg()
+    cg = G.synth.city_grid(3000, seed=12)
+    with G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=0.1) as g:
+        g.linearise()
+        blocks = g.edge_blocks()
+        g.assemble()
+        rp, ci, va, xi = g.csr()
+    ob, _ = oracle.se2_linearise(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1)
+    assert_bitwise(blocks, ob, "SE(2) blocks")
+    rp2, ci2, va2, xi2 = oracle.csr_build_anchor(3 * cg.n_poses, cg.edge_i, cg.edge_j, ob, 1e6)
+    assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2)
+    assert_bitwise(va, va2, "SE(2) Omega")
+    assert_bitwise(xi, xi2, "SE(2) xi")
+
+
+def test_se2_converges_to_ground_truth_scale():
+    G = load_pkg()
+    cg = G.synth.city_grid(2000, seed=13)
+    with G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=1.0,
+                              tol=1e-10, max_iter=100000, angle_wrap=1) as g:
+        d = [g.round().diff for _ in range(4)]
+        p = g.poses
+    err0 = np.abs(cg.init[:, :2] - cg.gt[:, :2]).max()
+    err = np.abs(p[:, :2] - cg.gt[:, :2]).max()
+    assert d[-1] < 1e-4 and err < err0
+
+
+# ---------------------------------------------------------------- edge cases
+
+def test_bad_observation_step_rejected():
+    """The reference indexes poses with the observation step and crashes on
+    cityTrees100_100 (steps from 9900); libgslam returns BAD_INPUT."""
+    G = load_pkg()
+    poses = np.zeros((5, 3)); u = np.zeros((5, 2))
+    with pytest.raises(G.abi.GslamError) as e:
+        G.PoseGraph.from_reference(poses, u, 1.0, 1.0, [0, 9], [7, 7], np.ones((2, 2)))
+    assert e.value.code == G.abi.ERR_BAD_INPUT
+
+
+def test_single_pose_and_two_poses(oracle):
+    G = load_pkg()
+    for n in (1, 2):
+        poses = np.zeros((n, 3)); u = np.zeros((n, 2)); u[:, 0] = 1.0; u[:, 1] = 0.1
+        with G.PoseGraph.from_reference(poses, u, 1.0, 1.0, [], [], np.zeros((0, 2))) as g:
+            g.linearise()
+            g.assemble()
+            rp, ci, va, xi = g.csr()
+            st = g.solve()
+        og = oracle.Graph(1.0, np.arange(n), u, np.arange(n), poses, [], [], np.zeros((0, 2)))
+        t1, t2, ob = oracle.linearise(og, poses, 1.0, cr=True)
+        rp2, ci2, va2, xi2 = oracle.csr_build(3 * n, t1, t2, ob)
+        assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2)
+        assert_bitwise(va, va2, f"n={n} Omega")
+
+
+def test_barrier_timeout_returns_status():
+    """A solver CTA that never arrives makes the others' bounded wait run out:
+    the call returns DEVICE_TIMEOUT and the context stays usable."""
+    G = load_pkg()
+    _, log, lam = cases()[1]
+    with G.PoseGraph.from_log(log, lam, ctas_per_sm=1, barrier_timeout_ms=20.0,
+                              test_absent_cta=1) as g:
+        g.linearise()
+        g.assemble()
+        with pytest.raises(G.abi.GslamError) as e:
+            g.solve()
+        assert e.value.code == G.abi.ERR_DEVICE_TIMEOUT
+        g.set_opts(test_absent_cta=-1)
+        st = g.solve()
+        assert st.reason in (G.abi.STOP_TOL, G.abi.STOP_MAXIT)
+
+
+# ---------------------------------------------------------------- drop-in ABI
+
+def test_dropin_device_graph(oracle):
+    """device_graph_init/update/pcg_solve (the reference GPU twin's API)."""
+    G = load_pkg()
+    A = G.abi
+    L = A.lib()
+    _, log, lam = cases()[2]
+    n = log.n_poses
+    zs = (A.ZRec * len(log.z_lm))()
+    for i in range(len(log.z_lm)):
+        zs[i].step = int(log.z_step[i]); zs[i].landmark_id = int(log.z_lm[i])
+        zs[i].z[0], zs[i].z[1] = log.z[i]
+    us = (A.URec * n)()
+    for i in range(n):
+        us[i].step = i; us[i].nu = log.u[i, 0]; us[i].omega = log.u[i, 1]
+    hx = (A.HatXRec * n)()
+    for i in range(n):
+        hx[i].step = i
+        hx[i].hat_x[0], hx[i].hat_x[1], hx[i].hat_x[2] = log.x[i]
+    mns = np.array([0.19, 0.001, 0.13, 0.2])
+    nnz = C.c_int()
+    os.environ["GSLAM_DROPIN_NOEXIT"] = "1"
+    L.device_graph_init(zs, len(log.z_lm), us, n, 3 * n, log.delta, lam, A.ptr(mns), C.byref(nnz))
+    assert L.gslam_dropin_status() == 0
+    d_vals = torch.zeros(nnz.value, dtype=torch.float64, device="cuda")
+    d_xi = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    L.device_graph_update(hx, n, C.c_void_p(d_vals.data_ptr()), C.c_void_p(d_xi.data_ptr()))
+    assert L.gslam_dropin_status() == 0
+    torch.cuda.synchronize()
+    og = _ograph(oracle, log)
+    t1, t2, ob = oracle.linearise(og, og.x, lam, cr=True)
+    rp, ci, va, xi = oracle.csr_build(og.dim, t1, t2, ob)
+    assert nnz.value == len(va)
+    assert_bitwise(d_vals.cpu().numpy(), va, "drop-in CSR values")
+    assert_bitwise(d_xi.cpu().numpy(), xi, "drop-in xi")
+    d_rp = L.device_graph_get_row_ptr()
+    h_rp = torch.empty(3 * n + 1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    x = np.zeros(3 * n)
+    L.device_pcg_solve(A.ptr(x), C.c_void_p(d_vals.data_ptr()), C.c_void_p(d_xi.data_ptr()),
+                       3 * n, nnz.value, 500)
+    assert L.gslam_dropin_status() == 0
+    x_ref, _, _ = oracle.pcg(rp, ci, va, xi)
+    assert np.linalg.norm(x - x_ref) <= 1e-3 * np.linalg.norm(x_ref)
+    assert d_rp is not None and h_rp is not None
+    L.device_graph_free()
+
+
+def test_dropin_pcg_solve_sparse(oracle):
+    """pcg_solve_sparse(x, CSRMatrix*, b, dim) with the reference's own CSR."""
+    G = load_pkg()
+    A = G.abi
+    L = A.lib()
+    _, log, lam = cases()[3]
+    og = _ograph(oracle, log)
+    t1, t2, ob = oracle.linearise(og, og.x, lam, cr=False)
+    rp, ci, va, xi = oracle.csr_build(og.dim, t1, t2, ob)
+    csr = A.CSRMatrix(A.ptr(rp, C.c_int), A.ptr(ci, C.c_int), A.ptr(va), og.dim, len(va))
+    os.environ["GSLAM_DROPIN_NOEXIT"] = "1"
+    outs = []
+    for _ in range(2):            # second call reuses the cached layout
+        x = np.zeros(og.dim)
+        L.pcg_solve_sparse(A.ptr(x), C.byref(csr), A.ptr(xi), og.dim)
+        assert L.gslam_dropin_status() == 0
+        outs.append(x)
+    x_ref, _, _ = oracle.pcg(rp, ci, va, xi)
+    assert_bitwise(outs[0], outs[1], "repeat")
+    assert np.linalg.norm(outs[0] - x_ref) <= 1e-3 * np.linalg.norm(x_ref)
+
+
+def test_cli_matches_reference_program(oracle, tmp_path):
+    """The GSLAM program: same stdout lines and header as the reference program,
+    same number of rounds, poses within tolerance of the oracle's run."""
+    G = load_pkg()
+    log = G.synth.landmark_log(800, seed=21)
+    path = str(tmp_path / "lm800.txt")
+    G.synth.write_log(path, log)
+    env = dict(os.environ, POSE_DUMP_FILE=str(tmp_path / "gpu.txt"), GSLAM_TOL="1e-10",
+               GSLAM_MAXIT="200000")
+    out = subprocess.run([G.abi.CLI_PATH, "1", "0.1", "5", "1", path], capture_output=True,
+                         text=True, env=env, check=True).stdout
+    lines = out.strip().splitlines()
+    assert lines[0] == f"Diff: 1 Lambda: 0.1 Rounds: 5 Drawing: 1 Input file: {path}"
+    assert lines[1] == (f"delta: 1.000000 size_of_us: {log.n_poses} size_of_hat_xs: {log.n_poses} "
+                        f"size_of_zlist: {len(log.z_lm)} dim: {3 * log.n_poses}")
+    og = _ograph(oracle, log)
+    p_ref, diffs, _ = oracle.run(og, 0.1, 5, cr=True, tol=1e-10, max_iter=200000)
+    rounds = [l for l in lines if "rounds executed" in l]
+    assert len(rounds) == len(diffs)
+    got = np.loadtxt(str(tmp_path / "gpu.txt"), ndmin=2)
+    assert np.array_equal(got[:, 0], np.arange(log.n_poses))
+    assert np.abs(got[:, 1:] - p_ref).max() <= 1e-7 * max(1.0, np.abs(p_ref).max())

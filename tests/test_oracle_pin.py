@@ -1,0 +1,115 @@
+"""Pins the C oracle against the reference itself.
+
+The reference's cpu_pcg_fp64 sources are compiled from their own tree into
+oracle/_ref (oracle/Makefile). The oracle's glibc flavour must reproduce that
+build bit for bit: edge blocks, CSR, xi, PCG output and whole multi-round runs.
+The committed fixtures under tests/golden (tests/golden/make_golden.py) pin the
+oracle on machines without the reference tree.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REF_DUMPS, assert_bitwise, load_pkg, ref_data
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _need_ref(oracle):
+    if not oracle.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+
+
+@pytest.mark.parametrize("name,lam", [("cityTrees100.log.txt", 0.1), ("cityTrees800.txt", 0.1),
+                                      ("cityTrees1k.log.txt", 1.0), ("victoria-park-100.log.txt", 0.06)])
+def test_one_round_bitwise(oracle, name, lam):
+    _need_ref(oracle)
+    g = oracle.read_log(ref_data(name))
+    t1, t2, blocks, (rp, ci, va), xi, dx = oracle.ref_round(g, g.x, lam)
+    a1, a2, ab = oracle.linearise(g, g.x, lam, cr=False)
+    assert np.array_equal(t1, a1) and np.array_equal(t2, a2)
+    assert_bitwise(ab, blocks, "edge blocks")
+    rp2, ci2, va2, xi2 = oracle.csr_build(g.dim, a1, a2, ab)
+    assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2)
+    assert_bitwise(va2, va, "CSR values")
+    assert_bitwise(xi2, xi, "xi")
+    x, it, _ = oracle.pcg(rp2, ci2, va2, xi2)
+    assert_bitwise(x, dx, "PCG solution")
+
+
+@pytest.mark.parametrize("name,lam,rounds", [("cityTrees100.log.txt", 0.1, 10), ("cityTrees800.txt", 0.1, 10),
+                                             ("cityTrees1k.log.txt", 1.0, 4)])
+def test_run_bitwise_vs_reference_program(oracle, tmp_path, name, lam, rounds):
+    _need_ref(oracle)
+    path = ref_data(name)
+    out, poses = oracle.ref_run_binary(path, lam, rounds, str(tmp_path / "dump.txt"))
+    g = oracle.read_log(path)
+    p2, diffs, _ = oracle.run(g, lam, rounds, cr=False)
+    assert_bitwise(p2, poses, "poses after the run")
+    last = [l for l in out.splitlines() if "rounds executed" in l][-1]
+    n, d = last.split(" rounds executed: ")
+    assert int(n) == len(diffs) and float(d) == diffs[-1]
+
+
+def test_synthetic_log_bitwise_vs_reference_program(oracle, tmp_path):
+    _need_ref(oracle)
+    G = load_pkg()
+    cg = G.synth.city_grid(300, seed=5)
+    log = G.synth.to_reference_log(cg)
+    path = str(tmp_path / "city300.txt")
+    G.synth.write_log(path, log)
+    out, poses = oracle.ref_run_binary(path, 0.1, 4, str(tmp_path / "dump.txt"))
+    g = oracle.read_log(path)
+    p2, diffs, _ = oracle.run(g, 0.1, 4, cr=False)
+    assert_bitwise(p2, poses, "poses")
+
+
+def test_reference_defect_above_21845_documented(oracle):
+    """The reference marker index wraps in 32 bits for dim > 65535; the oracle's
+    sorted-key structure does not (no reference run needed: pure index arithmetic)."""
+    dim = 3 * 21846
+    f = 3 * 21845
+    wrapped = ((f + 2) * dim + (f + 2)) & 0xFFFFFFFF
+    assert wrapped != (f + 2) * dim + (f + 2)
+    t1 = np.arange(21845, dtype=np.uint32)
+    t2 = t1 + 1
+    rp, ci, va, xi = oracle.csr_build(dim, t1, t2, np.zeros((t1.size, 42)))
+    assert rp[-1] == 9 * (3 * 21846 - 2) + 3 * 0  # tridiagonal block pattern
+    assert ci.max() == dim - 1
+
+
+@pytest.mark.skipif(not os.environ.get("GSLAM_SLOW"), reason="116 GN rounds at N=7120 (set GSLAM_SLOW=1)")
+def test_victoria_park_golden_dump(oracle):
+    """The committed reference dump of `GSLAM 1 1.0 200 1 victoria-park.log.txt`."""
+    path = ref_data("victoria-park.log.txt")
+    dump = os.path.join(REF_DUMPS, "cpu_pcg_fp64.txt")
+    if not os.path.exists(dump):
+        pytest.skip("reference dump not present")
+    g = oracle.read_log(path)
+    p, diffs, _ = oracle.run(g, 1.0, 200, cr=False)
+    ref = np.loadtxt(dump, ndmin=2)[:, 1:4]
+    assert len(diffs) == 116
+    assert_bitwise(p, ref, "Victoria Park poses")
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
+def test_golden_fixtures(oracle, path):
+    """Committed oracle outputs on seeded synthetic graphs still reproduce bit for bit."""
+    z = np.load(path)
+    g = oracle.Graph(float(z["delta"]), z["u_step"], z["u"], z["x_step"], z["x"], z["z_step"],
+                     z["z_lm"], z["z"])
+    lam = float(z["lam"])
+    for cr, key in ((False, "blocks_glibc"), (True, "blocks_cr")):
+        _, _, b = oracle.linearise(g, g.x, lam, cr=cr)
+        assert_bitwise(b, z[key], key)
+    t1, t2, b = oracle.linearise(g, g.x, lam, cr=False)
+    rp, ci, va, xi = oracle.csr_build(g.dim, t1, t2, b)
+    assert np.array_equal(rp, z["row_ptr"]) and np.array_equal(ci, z["col_idx"])
+    assert_bitwise(va, z["values"], "values")
+    assert_bitwise(xi, z["xi"], "xi")
+    x, _, _ = oracle.pcg(rp, ci, va, xi)
+    assert_bitwise(x, z["dx"], "dx")
+    p, _, _ = oracle.run(g, lam, int(z["rounds"]), cr=False)
+    assert_bitwise(p, z["poses_run"], "poses after run")
