@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Benchmark: Gauss-Newton iterations per second on a 100,000-pose graph.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the seeded city-grid SE(2) pose graph with 100,000 poses (1 m steps,
+20 m blocks, up to 3 loop closures per pose within 2 m and |dtheta| < 0.3 rad,
+odometry / closure noise 0.05 m / 0.01 rad, information diag(1/sigma^2) * 0.1,
+initial guess = composed odometry). One step = one Gauss-Newton iteration:
+linearise every edge, assemble Omega and xi, invert the 3x3 diagonal blocks,
+block-Jacobi PCG with the reference's per-round settings (||r|| < 1e-6 ||xi||
+or 500 iterations), add dx to the poses (angles wrapped).
+
+Our arm runs it through libgslam on the GPU; the reference arm runs the CPU
+oracle (the reference's algorithm restated in C, single thread) on the same
+workload. Under torchrun each rank solves its own seeded replica (weak
+scaling; one graph does not shard: see DESIGN.md).
+"""
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "g-slam_on_gpu_and_fpga_b200"
+
+N_POSES = 100000
+LAMBDA = 0.1
+TOL, MAX_ITER = 1e-6, 500
+METRIC = "GN iters/s at N=100k (block-Jacobi PCG per round: tol 1e-6, 500 iterations)"
+UNIT = "GN iters/s"
+
+
+def workload(seed):
+    G = importlib.import_module(PKG)
+    return G.synth.city_grid(N_POSES, seed=seed, k_closures=3, radius=2.0, max_dtheta=0.3)
+
+
+def config(extra=None):
+    c = {"workload": "city-grid SE(2) pose graph, N=100000, K=3 closures within 2 m, lambda=0.1; "
+                     "one Gauss-Newton round with block-Jacobi PCG (tol 1e-6, max 500 iterations)",
+         "n_poses": N_POSES, "lambda": LAMBDA, "pcg_tol": TOL, "pcg_max_iter": MAX_ITER,
+         "l2": "flushed between timed steps (256 MiB device write, outside the timed events)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# --------------------------------------------------------------------------- distributed
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def dist_init(world):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(dist, value):
+    if dist is None:
+        return value
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if sms:
+            out["sm_mhz"] = statistics.median(sms)
+            out["sm_max_mhz"] = mx
+            out["samples"] = len(sms)
+        out["reasons"] = sorted(reasons)
+        return out
+
+
+# --------------------------------------------------------------------------- roofline
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return json.load(open(path)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def pcg_bytes_per_iteration(nnzb, nb, s_a, s_v):
+    """Algorithmic bytes of one fused PCG iteration: SpMV (values, block columns, row
+    pointers, x read and y written once) + 5 vector streams + the FP64 3x3 inverses."""
+    b_spmv = nnzb * (9 * s_a + 4) + 4 * (nb + 1) + 2 * 3 * nb * s_v
+    return b_spmv + 5 * 3 * nb * s_v + 72 * nb
+
+
+def solver_traffic_per_iteration(arm):
+    """DRAM bytes per solver iteration from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"pcg_{arm}_n100k_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_iteration:"):
+            return float(line.split(":")[1])
+    return None
+
+
+# --------------------------------------------------------------------------- our arm
+
+def run_arm(G, torch, cg, precision, steps, warmup, flush):
+    g = G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=LAMBDA,
+                             tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=precision)
+    stream = torch.cuda.ExternalStream(g.stream())
+    for _ in range(warmup):
+        g.round()
+    sizes = g.sizes()
+    rounds, solves, iters = [], [], []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        st = g.round()
+        rounds.append(st.round_ms)
+        solves.append(st.solve_ms)
+        iters.append(st.iterations)
+    return g, stream, sizes, rounds, solves, iters
+
+
+def e2e_arm(G, torch, g, stream, steps):
+    """Same rounds through host buffers: pinned poses in, round, pinned poses out."""
+    n = g.n_poses
+    h_in = torch.from_numpy(g.poses).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    lib = G.abi.lib()
+    ptr_in = C.cast(h_in.data_ptr(), C.POINTER(C.c_double))
+    ptr_out = C.cast(h_out.data_ptr(), C.POINTER(C.c_double))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(steps):
+        ev0.record(stream)
+        G.abi.check(lib.gslam_set_poses(g._h, ptr_in))
+        g.round()
+        G.abi.check(lib.gslam_get_poses(g._h, ptr_out))
+        ev1.record(stream)
+        ev1.synchronize()
+        total += ev0.elapsed_time(ev1)
+        h_in.copy_(h_out)
+    return total, 3 * n * 8, 3 * n * 8
+
+
+def cpu_baseline_sample(cg, rounds=2):
+    """The oracle (reference algorithm in C, one thread) on the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle as O
+    O.build()
+    poses = cg.init.copy()
+    dim = 3 * cg.n_poses
+    t0 = time.perf_counter()
+    for _ in range(rounds):
+        blocks, _ = O.se2_linearise(poses, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAMBDA)
+        rp, ci, va, xi = O.csr_build_anchor(dim, cg.edge_i, cg.edge_j, blocks, 1e6)
+        dx, _, _ = O.pcg(rp, ci, va, xi, tol=TOL, max_iter=MAX_ITER)
+        poses = poses + dx.reshape(-1, 3)
+        poses[:, 2] = (poses[:, 2] + np.pi) % (2 * np.pi) - np.pi
+    dt = time.perf_counter() - t0
+    return rounds / dt, dt
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    dist = dist_init(world)
+    torch.cuda.set_device(local)
+    G = importlib.import_module(PKG)
+    G.build.build()
+    cg = workload(seed=1 + rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    peaks, peak_kind = measured_peaks()
+
+    results = {}
+    for arm, prec in (("fp64", G.abi.PREC_FP64),):
+        barrier(dist)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            g, stream, sizes, rounds, solves, iters = run_arm(G, torch, cg, prec, args.steps,
+                                                               args.warmup, flush)
+            torch.cuda.synchronize()
+        barrier(dist)
+        total_ms = max_over_ranks(dist, sum(rounds))
+        e2e_ms, h2d, d2h = e2e_arm(G, torch, g, stream, args.steps)
+        e2e_ms = max_over_ranks(dist, e2e_ms)
+        results[arm] = dict(g=g, sizes=sizes, rounds=rounds, solves=solves, iters=iters,
+                            total_ms=total_ms, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h, clocks=clk.summary())
+
+    r = results["fp64"]
+    s_a = s_v = 8
+    nb, nnzb = r["sizes"]["n_poses"], r["sizes"]["nnzb"]
+    b_iter = pcg_bytes_per_iteration(nnzb, nb, s_a, s_v)
+    mean_iters = statistics.mean(r["iters"])
+    mean_solve_ms = statistics.mean(r["solves"])
+    achieved = b_iter * mean_iters / (mean_solve_ms * 1e-3) / 1e9
+    traffic_it = solver_traffic_per_iteration("fp64")
+    value = world * args.steps / (r["total_ms"] * 1e-3)
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(r["total_ms"] / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded city-grid walk; no dataset)",
+        "config": config({"solver": "fp64 block-Jacobi PCG, matrix resident in shared memory",
+                          "nnzb": nnzb, "pcg_iterations_mean": mean_iters,
+                          "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
+        "roofline": {"kernel": "k_pcg64_res (persistent PCG solve)", "bound": "hbm",
+                     "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_iteration": b_iter,
+                     "traffic": (round(traffic_it * mean_iters) if traffic_it else None),
+                     "solve_ms_mean": round(mean_solve_ms, 4),
+                     "us_per_pcg_iteration": round(1e3 * mean_solve_ms / mean_iters, 3)},
+        "e2e": {"value": round(world * args.steps / (r["e2e_ms"] * 1e-3), 3), "unit": UNIT,
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": 7 * args.steps,
+        "clocks": r["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt = cpu_baseline_sample(cg)
+        line["cpu_baseline"] = {"value": round(v, 5), "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": f"2 GN rounds of the same N=100000 workload ({dt:.1f} s)"}
+    for arm in results.values():
+        arm["g"].close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    cg = workload(seed=1)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle as O
+    O.build()
+    dim = 3 * cg.n_poses
+    poses = cg.init.copy()
+
+    def one_round(p):
+        blocks, _ = O.se2_linearise(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAMBDA)
+        rp, ci, va, xi = O.csr_build_anchor(dim, cg.edge_i, cg.edge_j, blocks, 1e6)
+        dx, _, _ = O.pcg(rp, ci, va, xi, tol=TOL, max_iter=MAX_ITER)
+        p = p + dx.reshape(-1, 3)
+        p[:, 2] = (p[:, 2] + np.pi) % (2 * np.pi) - np.pi
+        return p
+
+    for _ in range(args.warmup):
+        poses = one_round(poses)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        poses = one_round(poses)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    line = {
+        "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded city-grid walk; no dataset)", "impl": "reference",
+        "config": config({"solver": "reference algorithm restated in C (oracle/), one host thread"}),
+        "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"{args.steps} GN rounds of the N=100000 workload"},
+        "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -30,10 +30,10 @@ STOP_TOL, STOP_MAXIT, STOP_PQ_ZERO, STOP_TIMEOUT = 0, 1, 2, 3
 # every extern "C" symbol the headers declare (checked by the CPU tests)
 EXPORTS = [
     "gslam_opts_default", "gslam_create_reference", "gslam_create_se2", "gslam_destroy",
-    "gslam_set_opts", "gslam_sizes", "gslam_set_poses", "gslam_get_poses", "gslam_round",
+    "gslam_set_opts", "gslam_sizes", "gslam_get_stream", "gslam_set_poses", "gslam_get_poses", "gslam_round",
     "gslam_run", "gslam_linearise", "gslam_assemble", "gslam_solve", "gslam_update",
     "gslam_get_edge_blocks", "gslam_assemble_from_edges", "gslam_get_csr", "gslam_get_dx",
-    "gslam_get_diag_inv", "gslam_spmv", "gslam_spmv_bench", "gslam_read_log", "gslam_free_log",
+    "gslam_get_diag_inv", "gslam_spmv", "gslam_spmv_bench", "gslam_spmv_bytes", "gslam_read_log", "gslam_free_log",
     "gslam_version", "gslam_last_error", "gslam_obs_edge_order", "gslam_csr_pattern",
     "pcg_solve_sparse", "device_graph_init", "device_graph_update", "device_graph_get_row_ptr",
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
@@ -52,12 +52,13 @@ class Opts(C.Structure):
                 ("sell_window", C.c_int), ("threads_per_cta", C.c_int), ("ctas_per_sm", C.c_int),
                 ("angle_wrap", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
                 ("max_refine", C.c_int), ("device", C.c_int), ("barrier_timeout_ms", C.c_double),
-                ("test_absent_cta", C.c_int)]
+                ("test_absent_cta", C.c_int), ("disable_resident", C.c_int)]
 
 
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("reason", C.c_int),
-                ("rel_residual", C.c_double), ("diff", C.c_double)]
+                ("rel_residual", C.c_double), ("diff", C.c_double), ("solve_ms", C.c_double),
+                ("round_ms", C.c_double)]
 
 
 class ReferenceGraphDesc(C.Structure):
@@ -121,6 +122,7 @@ def lib() -> C.CDLL:
             "gslam_destroy": [VP],
             "gslam_set_opts": [VP, C.POINTER(Opts)],
             "gslam_sizes": [VP, I64P, I64P, I64P, I64P],
+            "gslam_get_stream": [VP, C.POINTER(VP)],
             "gslam_set_poses": [VP, DP],
             "gslam_get_poses": [VP, DP],
             "gslam_round": [VP, C.POINTER(SolveStats)],
@@ -135,7 +137,8 @@ def lib() -> C.CDLL:
             "gslam_get_dx": [VP, DP],
             "gslam_get_diag_inv": [VP, DP],
             "gslam_spmv": [VP, VP, VP],
-            "gslam_spmv_bench": [VP, C.c_int, C.c_int, C.POINTER(C.c_float)],
+            "gslam_spmv_bench": [VP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)],
+            "gslam_spmv_bytes": [VP, C.c_int, I64P],
             "gslam_read_log": [C.c_char_p, C.POINTER(C.POINTER(LogDesc))],
             "gslam_free_log": [C.POINTER(LogDesc)],
             "gslam_obs_edge_order": [C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),

@@ -12,6 +12,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -23,8 +24,26 @@
 #include "gslam_api_internal.h"
 #include "gslam_internal.h"
 #include "kernels.cuh"
+#include "pcg_common.cuh"
 
 static thread_local std::string g_last_error;
+
+/* GSLAM_TRACE=1: host time of each step of a solve on stderr (diagnostics). */
+static bool trace_on() {
+    static int on = -1;
+    if (on < 0) on = getenv("GSLAM_TRACE") && atoi(getenv("GSLAM_TRACE")) ? 1 : 0;
+    return on == 1;
+}
+struct HostTrace {
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void step(const char *what) {
+        if (!trace_on()) return;
+        auto n = std::chrono::steady_clock::now();
+        fprintf(stderr, "[gslam trace] %-28s %9.1f us\n", what,
+                std::chrono::duration<double, std::micro>(n - t).count());
+        t = n;
+    }
+};
 
 void gslam_set_error(const char *fmt, const char *what, int code) {
     char buf[512];
@@ -68,6 +87,7 @@ int gslam_opts_default(gslam_opts *o) {
     o->device = -1;
     o->barrier_timeout_ms = 0.0;
     o->test_absent_cta = -1;
+    o->disable_resident = 0;
     return GSLAM_OK;
 }
 
@@ -132,7 +152,13 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
     /* solver launch shape */
     int n_sm = 0;
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
-    L->block = o.threads_per_cta ? o.threads_per_cta : 256;
+    {
+        int khz = 0;   /* this query costs milliseconds: once per layout, not per solve */
+        if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device) != cudaSuccess || khz <= 0)
+            khz = 2000000;
+        L->clock_khz = khz;
+    }
+    L->block = o.threads_per_cta ? o.threads_per_cta : 1024;
     int maxg = pcg_max_grid(GSLAM_PREC_FP64, L->block, device);
     if (maxg <= 0) {
         g_last_error = "persistent solver cannot be made co-resident at this block size";
@@ -145,9 +171,51 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
     L->grid = std::max(1, std::min(grid, needed));
     L->n_sm = n_sm;
     L->partial_capacity = std::max(L->grid, maxg);
+    /* resident solver: contiguous slice ranges per CTA balanced by slot count, at most
+     * one slice per warp (32 per CTA); values staged in shared memory up to its size */
+    L->resident = false;
+    const int rgrid = pcg_resident_max_grid(device, GSLAM_RES_SMEM_MAX);
+    if (!o.disable_resident && rgrid > 0 && S.n_slices <= 32 * rgrid) {
+        const int block = (S.n_slices <= 24 * rgrid) ? 768 : 1024;
+        const int cap_sl = block / 32;          /* one slice per warp */
+        /* boundaries at equal shares of the slot prefix sum, then clamped so that no
+         * CTA owns more than cap_sl slices (feasible since n_slices <= cap_sl * rgrid) */
+        std::vector<int> cs(rgrid + 1);
+        const int64_t total = S.n_slots;
+        int sl = 0;
+        for (int i = 0; i <= rgrid; i++) {
+            const int64_t want = total * i / rgrid;
+            while (sl < S.n_slices && S.slice_ptr[sl] < want) sl++;
+            cs[i] = sl;
+        }
+        cs[0] = 0;
+        cs[rgrid] = S.n_slices;
+        for (int i = 1; i <= rgrid; i++) cs[i] = std::min(std::max(cs[i], cs[i - 1]), cs[i - 1] + cap_sl);
+        cs[rgrid] = S.n_slices;
+        for (int i = rgrid - 1; i >= 0; i--) cs[i] = std::max(std::min(cs[i], cs[i + 1]), cs[i + 1] - cap_sl);
+        bool ok = cs[0] == 0;
+        int64_t max_slots = 0;
+        for (int i = 0; i < rgrid; i++) {
+            if (cs[i + 1] < cs[i] || cs[i + 1] - cs[i] > cap_sl) ok = false;
+            max_slots = std::max(max_slots, S.slice_ptr[cs[i + 1]] - S.slice_ptr[cs[i]]);
+        }
+        const int64_t col_bytes = (4 * max_slots + 127) / 128 * 128;
+        const int64_t cap = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes) / 8 / 288 * 288;
+        if (ok && cap >= 0) {
+            L->resident = true;
+            L->res_grid = rgrid;
+            L->res_block = block;
+            L->smem_val_cap = std::min<int64_t>(cap, 9 * max_slots);
+            L->smem_bytes = (size_t)(8 * L->smem_val_cap + 4 * max_slots);
+            CK(dupload(m, st, &L->cta_slice, cs));
+            L->partial_capacity = std::max(L->partial_capacity, rgrid);
+        }
+    }
     CK(dalloc(m, &L->partials, 8 * (size_t)L->partial_capacity));
     CK(dalloc(m, &L->gs, 1));
     CK(dalloc(m, &L->res, 1));
+    CK(cudaEventCreate(&L->ev0));
+    CK(cudaEventCreate(&L->ev1));
     return GSLAM_OK;
 }
 
@@ -173,8 +241,10 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
         int rc = gslam_layout_ensure_fp32(L, st);
         if (rc != GSLAM_OK) return rc;
     }
+    HostTrace tr;
     launch_diag_inv(st, L->n_rows, L->diag_slot, L->val, L->dinv);
     CK(cudaGetLastError());
+    tr.step("diag_inv launch");
     PcgParams P;
     memset(&P, 0, sizeof P);
     P.n_rows = L->n_rows;
@@ -197,21 +267,38 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
     P.gs = L->gs;
     P.res = L->res;
     {
-        /* barrier wait limit in SM clock cycles */
-        int khz = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev);
-        if (khz <= 0) khz = 2000000;
+        /* barrier wait limit in SM clock cycles (clock rate queried once at setup) */
         const double ms = o.barrier_timeout_ms > 0 ? o.barrier_timeout_ms : 2000.0;
-        P.spin_limit = (long long)(ms * (double)khz);
+        P.spin_limit = (long long)(ms * (double)L->clock_khz);
     }
     P.absent_cta = o.test_absent_cta;
     CK(cudaMemsetAsync(L->gs, 0, sizeof(GridSync), st));
     CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
-    CK(launch_pcg(st, P, fused_prec, L->grid, L->block));
+    const bool resident = L->resident && fused_prec == GSLAM_PREC_FP64 && !o.disable_resident;
+    const int grid = resident ? L->res_grid : L->grid;
+    {
+        /* 2 barriers per iteration + 1: the arrival counter must not wrap */
+        const double barriers = 2.0 * (double)std::max(o.max_iter, 0) + 4.0;
+        if (barriers * (double)grid >= 4294967295.0) {
+            g_last_error = "max_iter too large for the solver's 32-bit barrier counter";
+            return GSLAM_ERR_TOO_LARGE;
+        }
+    }
+    P.cta_slice = L->cta_slice;
+    P.smem_val_cap = L->smem_val_cap;
+    tr.step("memsets");
+    CK(cudaEventRecord(L->ev0, st));
+    if (resident) CK(launch_pcg_resident(st, P, grid, L->res_block, L->smem_bytes));
+    else CK(launch_pcg(st, P, fused_prec, grid, L->block));
+    tr.step("solver launch");
+    CK(cudaEventRecord(L->ev1, st));
     CK(cudaMemcpyAsync(h_res, L->res, sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    tr.step("solver wait");
+    float solve_ms = 0.f;
+    cudaEventElapsedTime(&solve_ms, L->ev0, L->ev1);
     if (stats) {
+        stats->solve_ms = solve_ms;
         stats->iterations = h_res->iterations;
         stats->refinements = h_res->refinements;
         stats->reason = h_res->reason;
@@ -224,7 +311,12 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
     return GSLAM_OK;
 }
 
-void gslam_layout_release(DevLayout *L) { L->mem.release(); }
+void gslam_layout_release(DevLayout *L) {
+    L->mem.release();
+    if (L->ev0) cudaEventDestroy(L->ev0);
+    if (L->ev1) cudaEventDestroy(L->ev1);
+    L->ev0 = L->ev1 = nullptr;
+}
 
 /* ------------------------------------------------------------------------ */
 /* graph creation                                                            */
@@ -232,7 +324,7 @@ void gslam_layout_release(DevLayout *L) { L->mem.release(); }
 
 static int common_setup(gslam_graph *g, const gslam_opts *opts) {
     if (opts) g->o = *opts; else gslam_opts_default(&g->o);
-    if (g->o.sell_window <= 0) g->o.sell_window = 256;
+    if (g->o.sell_window <= 0) g->o.sell_window = 1024;
     if (g->o.device >= 0) CK(cudaSetDevice(g->o.device));
     CK(cudaGetDevice(&g->device));
     CK(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
@@ -365,6 +457,8 @@ int gslam_destroy(gslam_graph *g) {
     g->mem.release();
     if (g->h_res) cudaFreeHost(g->h_res);
     if (g->h_diff) cudaFreeHost(g->h_diff);
+    if (g->ev_round0) cudaEventDestroy(g->ev_round0);
+    if (g->ev_round1) cudaEventDestroy(g->ev_round1);
     if (g->st) cudaStreamDestroy(g->st);
     delete g;
     return GSLAM_OK;
@@ -470,29 +564,47 @@ int gslam_solve(gslam_graph *g, gslam_solve_stats *stats) {
     return rc;
 }
 
-int gslam_update(gslam_graph *g, double *diff) {
+int gslam_update(gslam_graph *g, double *diff) { return gslam_update_ex(g, diff, nullptr); }
+
+int gslam_update_ex(gslam_graph *g, double *diff, cudaEvent_t done) {
     if (!g) BAD("null handle");
     launch_pose_update(g->st, g->n_poses, g->L.iperm, g->L.x4, g->d_poses, g->d_dx, g->o.angle_wrap,
                        g->d_block_sums, g->n_upd_blocks, g->d_diff);
     CK(cudaGetLastError());
+    if (done) CK(cudaEventRecord(done, g->st));
     CK(cudaMemcpyAsync(g->h_diff, g->d_diff, sizeof(double), cudaMemcpyDeviceToHost, g->st));
     CK(cudaStreamSynchronize(g->st));
     if (diff) *diff = *g->h_diff;
     return GSLAM_OK;
 }
 
+int gslam_get_stream(gslam_graph *g, void **stream) {
+    if (!g || !stream) BAD("null argument");
+    *stream = (void *)g->st;
+    return GSLAM_OK;
+}
+
 int gslam_round(gslam_graph *g, gslam_solve_stats *stats) {
     if (!g) BAD("null handle");
+    if (!g->ev_round0) {
+        CK(cudaEventCreate(&g->ev_round0));
+        CK(cudaEventCreate(&g->ev_round1));
+    }
+    CK(cudaEventRecord(g->ev_round0, g->st));
     int rc = gslam_linearise(g);
     if (rc != GSLAM_OK) return rc;
     rc = gslam_assemble(g);
     if (rc != GSLAM_OK) return rc;
     gslam_solve_stats st;
+    memset(&st, 0, sizeof st);
     rc = gslam_solve(g, &st);
     if (rc != GSLAM_OK) { if (stats) *stats = st; return rc; }
     double diff = 0.0;
-    rc = gslam_update(g, &diff);
+    rc = gslam_update_ex(g, &diff, g->ev_round1);
     st.diff = diff;
+    float ms = 0.f;
+    if (rc == GSLAM_OK) cudaEventElapsedTime(&ms, g->ev_round0, g->ev_round1);
+    st.round_ms = ms;
     if (stats) *stats = st;
     return rc;
 }
@@ -584,30 +696,69 @@ int gslam_spmv(gslam_graph *g, const double *d_x, double *d_y) {
     return GSLAM_OK;
 }
 
-int gslam_spmv_bench(gslam_graph *g, int prec, int reps, float *ms) {
-    if (!g || !ms || reps <= 0) BAD("bad argument");
+int gslam_spmv_bench(gslam_graph *g, int prec, int reps, int n_copies, float *ms) {
+    if (!g || !ms || reps <= 0 || n_copies <= 0) BAD("bad argument");
     if (prec == 1) {
         int rc = gslam_layout_ensure_fp32(&g->L, g->st);
         if (rc != GSLAM_OK) return rc;
     }
-    cudaEvent_t a, b;
-    CK(cudaEventCreate(&a));
-    CK(cudaEventCreate(&b));
-    CK(cudaEventRecord(a, g->st));
-    for (int i = 0; i < reps; i++) {
-        if (prec == 1)
-            launch_spmv32(g->st, g->n_poses, g->L.n_slices, g->L.slice_ptr, g->L.row_len, g->L.col,
-                          g->L.val32, g->L.f[3], g->L.f[5]);
-        else
-            launch_spmv64(g->st, g->n_poses, g->L.n_slices, g->L.slice_ptr, g->L.row_len, g->L.col,
-                          g->L.val, g->L.p4a, g->L.q4);
+    DevLayout &L = g->L;
+    const size_t nv = 9 * (size_t)L.n_slots;
+    const size_t esz = prec == 1 ? sizeof(float) : sizeof(double);
+    std::vector<void *> copies;
+    copies.push_back(prec == 1 ? (void *)L.val32 : (void *)L.val);
+    int rc = GSLAM_OK;
+    for (int c = 1; c < n_copies; c++) {
+        void *q = nullptr;
+        if (cudaMalloc(&q, nv * esz) != cudaSuccess) { rc = GSLAM_ERR_CUDA; break; }
+        copies.push_back(q);
+        cudaMemcpyAsync(q, copies[0], nv * esz, cudaMemcpyDeviceToDevice, g->st);
     }
-    CK(cudaEventRecord(b, g->st));
-    CK(cudaEventSynchronize(b));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
     float t = 0.f;
-    CK(cudaEventElapsedTime(&t, a, b));
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    *ms = t / reps;
+    if (rc == GSLAM_OK) {
+        cudaStreamSynchronize(g->st);
+        cudaError_t e = cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal);
+        for (int i = 0; i < reps && e == cudaSuccess; i++) {
+            const void *v = copies[i % copies.size()];
+            if (prec == 1)
+                launch_spmv32(g->st, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col,
+                              (const float *)v, L.f[3], L.f[5]);
+            else
+                launch_spmv64(g->st, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col,
+                              (const double *)v, L.p4a, L.q4);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(g->st, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->st);      /* warm-up replay */
+        if (e == cudaSuccess) e = cudaEventCreate(&a);
+        if (e == cudaSuccess) e = cudaEventCreate(&b);
+        if (e == cudaSuccess) e = cudaEventRecord(a, g->st);
+        if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->st);
+        if (e == cudaSuccess) e = cudaEventRecord(b, g->st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+        if (e != cudaSuccess) {
+            g_last_error = std::string("spmv bench: ") + cudaGetErrorString(e);
+            rc = GSLAM_ERR_CUDA;
+        }
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (size_t c = 1; c < copies.size(); c++) cudaFree(copies[c]);
+    if (rc == GSLAM_OK) *ms = t / reps;
+    return rc;
+}
+
+int gslam_spmv_bytes(gslam_graph *g, int prec, int64_t *bytes) {
+    if (!g || !bytes) BAD("null argument");
+    const int64_t sv = prec == 1 ? 4 : 8;
+    /* values + one column index per block + x read once + y written once (3 values/row) */
+    *bytes = g->S.nnzb * (9 * sv + 4) + 2 * 3 * (int64_t)g->n_poses * sv;
     return GSLAM_OK;
 }

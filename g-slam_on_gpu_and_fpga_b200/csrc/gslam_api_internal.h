@@ -34,7 +34,15 @@ struct DevLayout {
     GridSync *gs = nullptr;
     PcgResult *res = nullptr;
     int grid = 0, block = 0, n_sm = 0;
+    int clock_khz = 2000000;       /* SM clock, for barrier wait limits */
     int partial_capacity = 0;
+    /* shared-memory-resident solver (pcg_resident.cu), when the layout fits */
+    bool resident = false;
+    int res_grid = 0, res_block = 0;
+    int *cta_slice = nullptr;      /* [res_grid + 1] */
+    int64_t smem_val_cap = 0;      /* doubles staged per CTA */
+    size_t smem_bytes = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;   /* brackets the solver launch */
     int max_grid_alloc() const { return partial_capacity; }
 };
 
@@ -65,6 +73,7 @@ struct gslam_graph {
     PcgResult *h_res = nullptr;
     double *h_diff = nullptr;
     PcgResult last_res = {};
+    cudaEvent_t ev_round0 = nullptr, ev_round1 = nullptr;
 };
 
 int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st, int device,
@@ -76,6 +85,8 @@ void gslam_layout_release(DevLayout *L);
 /* Assembles Omega / xi from edge blocks; optionally also writes the reference's CSR
  * values (csr_vals) and xi in original order (xi_orig), both device pointers. */
 int gslam_assemble_ex(gslam_graph *g, const double *blocks, double *csr_vals, double *xi_orig);
+/* gslam_update that also records `done` (may be null) after the update kernels. */
+int gslam_update_ex(gslam_graph *g, double *diff, cudaEvent_t done);
 /* Records an error message for gslam_last_error(). */
 void gslam_set_last_error(const char *msg);
 void gslam_set_error(const char *fmt, const char *what, int code);

@@ -74,12 +74,19 @@ struct PcgParams {
     PcgResult *res;
     long long spin_limit;  /* clock cycles a barrier may wait */
     int absent_cta;        /* test hook: CTA that leaves before its first barrier, -1 = none */
+    const int *cta_slice;  /* resident solver: [grid + 1] first slice of each CTA */
+    int64_t smem_val_cap;  /* resident solver: values (multiple of 288) staged in shared memory */
 };
 
 /* Cooperative launch of the persistent solver; returns the CUDA error. */
 cudaError_t launch_pcg(cudaStream_t st, const PcgParams &p, int precision, int grid, int block);
 /* Largest co-resident grid for the solver at this block size (0 if unsupported). */
 int pcg_max_grid(int precision, int block, int device);
+
+/* Shared-memory-resident solver (pcg_resident.cu). */
+cudaError_t launch_pcg_resident(cudaStream_t st, const PcgParams &p, int grid, int block,
+                                size_t smem_bytes);
+int pcg_resident_max_grid(int device, size_t smem_bytes);
 
 /* Standalone SpMV y = A x on padded new-order vectors (FP64 or FP32 values). */
 void launch_spmv64(cudaStream_t st, int n_rows, int n_slices, const int64_t *slice_ptr,

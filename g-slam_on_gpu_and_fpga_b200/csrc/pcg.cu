@@ -26,142 +26,49 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "gslam.h"
 #include "kernels.cuh"
+#include "pcg_common.cuh"
 
 /* ------------------------------------------------------------------------ */
 /* grid barrier                                                              */
 /* ------------------------------------------------------------------------ */
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-__device__ __forceinline__ int ld_relaxed_s32(const int *p) {
-    int v;
-    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-/* Returns false when the solve must be abandoned (timeout here or elsewhere). */
-__device__ __forceinline__ bool grid_barrier(GridSync *gs, long long spin_limit, int *s_ok) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        __threadfence();
-        const unsigned gen = ld_acquire_u32(&gs->gen);
-        const unsigned arrived = atomicAdd(&gs->count, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            atomicExch(&gs->count, 0u);
-            __threadfence();
-            st_release_u32(&gs->gen, gen + 1u);
-        } else {
-            const long long t0 = clock64();
-            while (ld_acquire_u32(&gs->gen) == gen) {
-                if (ld_relaxed_s32(&gs->abort)) { ok = 0; break; }
-                if (clock64() - t0 > spin_limit) {
-                    atomicExch(&gs->abort, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
-
-/*
- * Deterministic all-reduce of NV doubles across the grid. v[] holds this
- * thread's partials on entry and the grid totals on exit.
- */
-template <int NV, int BS>
-__device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials_base, int &epoch,
-                                               GridSync *gs, long long spin_limit,
-                                               double (*s_red)[BS / 32], double *s_bc, int *s_ok) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    /* Two partial buffers alternate: a CTA can be at most one reduction ahead of
-     * the slowest reader, so it never overwrites partials still being summed. */
-    double *partials = partials_base + (epoch & 1) * 4 * gridDim.x;
-    epoch++;
-#pragma unroll
-    for (int i = 0; i < NV; i++) {
-        double a = v[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a = a + __shfl_down_sync(0xffffffffu, a, o);
-        if (lane == 0) s_red[i][warp] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < NV) {
-        double s = 0.0;
-#pragma unroll
-        for (int w = 0; w < BS / 32; w++) s = s + s_red[threadIdx.x][w];
-        partials[threadIdx.x * gridDim.x + blockIdx.x] = s;
-    }
-    if (!grid_barrier(gs, spin_limit, s_ok)) return false;
-    if (warp == 0) {
-#pragma unroll
-        for (int i = 0; i < NV; i++) {
-            double s = 0.0;
-            for (int c = lane; c < (int)gridDim.x; c += 32) s = s + partials[i * gridDim.x + c];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) s_bc[i] = s;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < NV; i++) v[i] = s_bc[i];
-    return true;
-}
-
 /* ------------------------------------------------------------------------ */
 /* FP64 persistent PCG                                                       */
 /* ------------------------------------------------------------------------ */
 
-struct V3 { double a, b, c; };
-
-__device__ __forceinline__ V3 ld3(const double *v4, int row) {
-    const double2 lo = *reinterpret_cast<const double2 *>(v4 + 4 * (size_t)row);
-    const double hi = v4[4 * (size_t)row + 2];
-    return V3{ lo.x, lo.y, hi };
+/*
+ * One row of q = A p with p formed on the fly from z and the previous p. Two
+ * blocks per step so both columns' gathers are in flight together; blocks are
+ * still added in ascending column order.
+ */
+__device__ __forceinline__ V3 spmv_row(const double *vb, const int *cb, int len, const double *z4,
+                                       const double *pold, double beta, bool first) {
+    double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+    int j = 0;
+    for (; j + 1 < len; j += 2) {
+        const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
+        const V3 p0 = p_of(z4, pold, c0, beta, first);
+        const V3 p1 = p_of(z4, pold, c1, beta, first);
+        blk_acc(vb + 288 * j, p0, q0, q1, q2);
+        blk_acc(vb + 288 * (j + 1), p1, q0, q1, q2);
+    }
+    if (j < len) {
+        const int c0 = __ldg(cb + 32 * j);
+        blk_acc(vb + 288 * j, p_of(z4, pold, c0, beta, first), q0, q1, q2);
+    }
+    return V3{ q0, q1, q2 };
 }
 
-__device__ __forceinline__ void st3(double *v4, int row, V3 v) {
-    *reinterpret_cast<double2 *>(v4 + 4 * (size_t)row) = make_double2(v.a, v.b);
-    v4[4 * (size_t)row + 2] = v.c;
-}
-
-/* p_new = z + beta * p_old exactly as MatrixOps.c:382 (first iteration: p = z). */
-__device__ __forceinline__ V3 p_of(const double *z4, const double *pold4, int row, double beta,
-                                   bool first) {
-    V3 z = ld3(z4, row);
-    if (first) return z;
-    V3 p = ld3(pold4, row);
-    return V3{ z.a + beta * p.a, z.b + beta * p.b, z.c + beta * p.c };
-}
-
-/* z = D^-1 r: z_i = ((0 + d_i0 r0) + d_i1 r1) + d_i2 r2 (MatrixOps.c:369-377). */
-__device__ __forceinline__ V3 apply_dinv(const double *dinv, int row, V3 r) {
-    const double *d = dinv + 288 * (size_t)(row >> 5) + (row & 31);
-    double z0 = 0.0, z1 = 0.0, z2 = 0.0;
-    z0 = z0 + d[0] * r.a;   z0 = z0 + d[32] * r.b;  z0 = z0 + d[64] * r.c;
-    z1 = z1 + d[96] * r.a;  z1 = z1 + d[128] * r.b; z1 = z1 + d[160] * r.c;
-    z2 = z2 + d[192] * r.a; z2 = z2 + d[224] * r.b; z2 = z2 + d[256] * r.c;
-    return V3{ z0, z1, z2 };
-}
-
-template <int BS>
-__global__ void __launch_bounds__(BS) k_pcg64(PcgParams P) {
+/*
+ * ONE: every warp owns at most one slice, so a row's p and q stay in registers
+ * from phase A to phase B; otherwise they go through memory.
+ */
+template <int BS, bool ONE>
+__global__ void __launch_bounds__(BS, 1) k_pcg64(PcgParams P) {
     __shared__ double s_red[3][BS / 32];
     __shared__ double s_bc[4];
     __shared__ int s_ok;
@@ -173,12 +80,12 @@ __global__ void __launch_bounds__(BS) k_pcg64(PcgParams P) {
      * other CTA's first barrier runs out of time and the solve reports a timeout. */
     if ((int)blockIdx.x == P.absent_cta) return;
 
-    /* x = 0, r = b, z = D^-1 r, p.. (MatrixOps.c:322-345) */
+    /* x = 0, r = b, z = D^-1 r (MatrixOps.c:322-345) */
     double acc2[2] = { 0.0, 0.0 };
     for (int s = gw; s < P.n_slices; s += TW) {
         const int row = 32 * s + lane;
         if (row >= P.n_rows) continue;
-        const V3 b = ld3(P.b4, row);
+        const V3 b = ldg3(P.b4, row);
         st3(P.x4, row, V3{ 0.0, 0.0, 0.0 });
         st3(P.r4, row, b);
         const V3 z = apply_dinv(P.dinv, row, b);
@@ -196,6 +103,20 @@ __global__ void __launch_bounds__(BS) k_pcg64(PcgParams P) {
     double beta = 0.0, rr = acc2[1];
     int k = 0, reason = GSLAM_STOP_MAXIT;
 
+    /* ONE-path row state */
+    const int my_row = 32 * gw + lane;
+    const bool mine = ONE && gw < P.n_slices && my_row < P.n_rows;
+    int my_len = 0;
+    const double *my_vb = nullptr;
+    const int *my_cb = nullptr;
+    if (mine) {
+        my_len = __ldg(P.row_len + my_row);
+        const int64_t sb = __ldg(P.slice_ptr + gw);
+        my_vb = P.val + 9 * sb + lane;
+        my_cb = P.col + sb + lane;
+    }
+    V3 pn_r = { 0.0, 0.0, 0.0 }, q_r = { 0.0, 0.0, 0.0 };
+
     while (true) {
         if (k >= P.max_iter) { reason = GSLAM_STOP_MAXIT; break; }
         const bool first = (k == 0);
@@ -203,26 +124,25 @@ __global__ void __launch_bounds__(BS) k_pcg64(PcgParams P) {
         const double *pold = (k & 1) ? P.p4a : P.p4b;
         /* ---- phase A: p, q = A p, p.q ---- */
         double pq[1] = { 0.0 };
-        for (int s = gw; s < P.n_slices; s += TW) {
-            const int row = 32 * s + lane;
-            if (row >= P.n_rows) continue;
-            const V3 pn = p_of(P.z4, pold, row, beta, first);
-            st3(pnew, row, pn);
-            const int len = P.row_len[row];
-            const int64_t sb = P.slice_ptr[s];
-            const double *vb = P.val + 9 * sb + lane;
-            const int *cb = P.col + sb + lane;
-            double q0 = 0.0, q1 = 0.0, q2 = 0.0;
-            for (int j = 0; j < len; j++) {
-                const int c = cb[32 * j];
-                const double *v = vb + 288 * j;
-                const V3 pc = p_of(P.z4, pold, c, beta, first);
-                q0 = q0 + v[0] * pc.a;   q0 = q0 + v[32] * pc.b;  q0 = q0 + v[64] * pc.c;
-                q1 = q1 + v[96] * pc.a;  q1 = q1 + v[128] * pc.b; q1 = q1 + v[160] * pc.c;
-                q2 = q2 + v[192] * pc.a; q2 = q2 + v[224] * pc.b; q2 = q2 + v[256] * pc.c;
+        if (ONE) {
+            if (mine) {
+                pn_r = p_of(P.z4, pold, my_row, beta, first);
+                st3(pnew, my_row, pn_r);
+                q_r = spmv_row(my_vb, my_cb, my_len, P.z4, pold, beta, first);
+                pq[0] = pq[0] + pn_r.a * q_r.a; pq[0] = pq[0] + pn_r.b * q_r.b; pq[0] = pq[0] + pn_r.c * q_r.c;
             }
-            st3(P.q4, row, V3{ q0, q1, q2 });
-            pq[0] = pq[0] + pn.a * q0; pq[0] = pq[0] + pn.b * q1; pq[0] = pq[0] + pn.c * q2;
+        } else {
+            for (int s = gw; s < P.n_slices; s += TW) {
+                const int row = 32 * s + lane;
+                if (row >= P.n_rows) continue;
+                const V3 pn = p_of(P.z4, pold, row, beta, first);
+                st3(pnew, row, pn);
+                const int64_t sb = __ldg(P.slice_ptr + s);
+                const V3 q = spmv_row(P.val + 9 * sb + lane, P.col + sb + lane, __ldg(P.row_len + row),
+                                      P.z4, pold, beta, first);
+                st3(P.q4, row, q);
+                pq[0] = pq[0] + pn.a * q.a; pq[0] = pq[0] + pn.b * q.b; pq[0] = pq[0] + pn.c * q.c;
+            }
         }
         if (!grid_allreduce<1, BS>(pq, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
             reason = GSLAM_STOP_TIMEOUT;
@@ -232,11 +152,11 @@ __global__ void __launch_bounds__(BS) k_pcg64(PcgParams P) {
         const double alpha = rz / pq[0];
         /* ---- phase B: x, r, z, r.r, r.z ---- */
         double rs[2] = { 0.0, 0.0 };
-        for (int s = gw; s < P.n_slices; s += TW) {
+        for (int s = gw; s < (ONE ? min(gw + 1, P.n_slices) : P.n_slices); s += TW) {
             const int row = 32 * s + lane;
             if (row >= P.n_rows) continue;
-            const V3 pn = ld3(pnew, row);
-            const V3 q = ld3(P.q4, row);
+            const V3 pn = ONE ? pn_r : ld3(pnew, row);
+            const V3 q = ONE ? q_r : ld3(P.q4, row);
             V3 x = ld3(P.x4, row), r = ld3(P.r4, row);
             x.a = x.a + alpha * pn.a; x.b = x.b + alpha * pn.b; x.c = x.c + alpha * pn.c;
             r.a = r.a - alpha * q.a;  r.b = r.b - alpha * q.b;  r.c = r.c - alpha * q.c;
@@ -265,7 +185,7 @@ __global__ void __launch_bounds__(BS) k_pcg64(PcgParams P) {
         P.res->iterations = k;
         P.res->reason = reason;
         P.res->refinements = 0;
-        P.res->timeout = (reason == GSLAM_STOP_TIMEOUT);
+        P.res->timeout = 0;
         P.res->rnorm = sqrt(rr);
         P.res->bnorm = bnorm;
     }
@@ -284,20 +204,10 @@ __global__ void k_spmv64(int n_rows, int n_slices, const int64_t *__restrict__ s
     if (s >= n_slices) return;
     const int row = 32 * s + lane;
     if (row >= n_rows) return;
-    const int len = row_len[row];
-    const int64_t sb = slice_ptr[s];
-    const double *vb = val + 9 * sb + lane;
-    const int *cb = col + sb + lane;
-    double q0 = 0.0, q1 = 0.0, q2 = 0.0;
-    for (int j = 0; j < len; j++) {
-        const int c = cb[32 * j];
-        const double *v = vb + 288 * j;
-        const V3 pc = ld3(x4, c);
-        q0 = q0 + v[0] * pc.a;   q0 = q0 + v[32] * pc.b;  q0 = q0 + v[64] * pc.c;
-        q1 = q1 + v[96] * pc.a;  q1 = q1 + v[128] * pc.b; q1 = q1 + v[160] * pc.c;
-        q2 = q2 + v[192] * pc.a; q2 = q2 + v[224] * pc.b; q2 = q2 + v[256] * pc.c;
-    }
-    st3(y4, row, V3{ q0, q1, q2 });
+    const int len = __ldg(row_len + row);
+    const int64_t sb = __ldg(slice_ptr + s);
+    /* p_of with first = true reads x4 only: q = A x */
+    st3(y4, row, spmv_row(val + 9 * sb + lane, col + sb + lane, len, x4, x4, 0.0, true));
 }
 
 __global__ void k_spmv32(int n_rows, int n_slices, const int64_t *__restrict__ slice_ptr,
@@ -330,35 +240,38 @@ __global__ void k_spmv32(int n_rows, int n_slices, const int64_t *__restrict__ s
 /* ------------------------------------------------------------------------ */
 
 template <int BS>
-static cudaError_t launch_pcg_bs(cudaStream_t st, const PcgParams &p, int precision, int grid) {
-    PcgParams copy = p;
-    void *args[] = { &copy };
-    (void)precision;
-    return cudaLaunchCooperativeKernel((const void *)k_pcg64<BS>, dim3(grid), dim3(BS), args, 0, st);
+static const void *pcg_fn(bool one) {
+    return one ? (const void *)k_pcg64<BS, true> : (const void *)k_pcg64<BS, false>;
+}
+
+static const void *pcg_kernel(int block, bool one) {
+    switch (block) {
+        case 256: return pcg_fn<256>(one);
+        case 512: return pcg_fn<512>(one);
+        case 1024: return pcg_fn<1024>(one);
+        default: return nullptr;
+    }
 }
 
 cudaError_t launch_pcg(cudaStream_t st, const PcgParams &p, int precision, int grid, int block) {
-    switch (block) {
-        case 128: return launch_pcg_bs<128>(st, p, precision, grid);
-        case 256: return launch_pcg_bs<256>(st, p, precision, grid);
-        case 512: return launch_pcg_bs<512>(st, p, precision, grid);
-        default: return cudaErrorInvalidValue;
-    }
+    (void)precision;
+    const bool one = (int64_t)grid * (block / 32) >= p.n_slices;
+    const void *fn = pcg_kernel(block, one);
+    if (!fn) return cudaErrorInvalidValue;
+    PcgParams copy = p;
+    void *args[] = { &copy };
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, 0, st);
 }
 
 int pcg_max_grid(int precision, int block, int device) {
     (void)precision;
-    int n_sm = 0, per_sm = 0;
+    int n_sm = 0, per_sm = 0, per_sm2 = 0;
     if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    const void *fn = nullptr;
-    switch (block) {
-        case 128: fn = (const void *)k_pcg64<128>; break;
-        case 256: fn = (const void *)k_pcg64<256>; break;
-        case 512: fn = (const void *)k_pcg64<512>; break;
-        default: return 0;
-    }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0) != cudaSuccess) return 0;
-    return per_sm * n_sm;
+    const void *f1 = pcg_kernel(block, true), *f2 = pcg_kernel(block, false);
+    if (!f1 || !f2) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f1, block, 0) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, f2, block, 0) != cudaSuccess) return 0;
+    return std::min(per_sm, per_sm2) * n_sm;
 }
 
 void launch_spmv64(cudaStream_t st, int n_rows, int n_slices, const int64_t *slice_ptr,

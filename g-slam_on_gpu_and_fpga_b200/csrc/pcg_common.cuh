@@ -1,0 +1,175 @@
+/* pcg_common.cuh — device pieces shared by the solver kernels (internal). */
+#ifndef GSLAM_PCG_COMMON_CUH
+#define GSLAM_PCG_COMMON_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.cuh"
+
+/* largest dynamic shared memory the resident solver asks for (sm_100: 227 KB per block) */
+#define GSLAM_RES_SMEM_MAX (225 * 1024)
+
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned atom_add_release_u32(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_relaxed_s32(const int *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+/*
+ * Grid barrier on a monotonic arrival counter: barrier number `epoch` (1, 2, ...)
+ * is complete when the counter reaches epoch * gridDim.x. One release atomic per
+ * CTA (it orders the CTA's prior writes, made visible to thread 0 by the CTA
+ * barrier), then acquire polling: the cheapest of the variants measured on B200
+ * (about 2.1 us per grid reduction with 148 CTAs, including the partials read). The counter is zeroed before every launch, so
+ * 2^32 / gridDim.x barriers fit in one solve. Returns false when the solve must be
+ * abandoned (this wait ran out of time, or another CTA's did).
+ */
+__device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned epoch, long long spin_limit,
+                                             int *s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned target = epoch * gridDim.x;
+        const unsigned arrived = atom_add_release_u32(&gs->count, 1u) + 1u;
+        if (arrived < target) {
+            const long long t0 = clock64();
+            while (ld_acquire_u32(&gs->count) < target) {
+                if (ld_relaxed_s32(&gs->abort)) { ok = 0; break; }
+                if (clock64() - t0 > spin_limit) {
+                    atomicExch(&gs->abort, 1);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+/*
+ * Deterministic all-reduce of NV doubles across the grid. v[] holds this
+ * thread's partials on entry and the grid totals on exit.
+ */
+template <int NV, int BS>
+__device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials_base, int &epoch,
+                                               GridSync *gs, long long spin_limit,
+                                               double (*s_red)[BS / 32], double *s_bc, int *s_ok) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    /* Two partial buffers alternate: a CTA can be at most one reduction ahead of
+     * the slowest reader, so it never overwrites partials still being summed. */
+    double *partials = partials_base + (epoch & 1) * 4 * gridDim.x;
+    epoch++;                                   /* this reduction's barrier number */
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+        double a = v[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a = a + __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) s_red[i][warp] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < BS / 32; w++) s = s + s_red[threadIdx.x][w];
+        partials[threadIdx.x * gridDim.x + blockIdx.x] = s;
+    }
+    if (!grid_barrier(gs, (unsigned)epoch, spin_limit, s_ok)) return false;
+    if (warp == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            double s = 0.0;
+            for (int c = lane; c < (int)gridDim.x; c += 32) s = s + __ldcg(partials + i * gridDim.x + c);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0) s_bc[i] = s;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NV; i++) v[i] = s_bc[i];
+    return true;
+}
+
+struct V3 { double a, b, c; };
+
+__device__ __forceinline__ V3 ld3(const double *v4, int row) {
+    const double2 lo = *reinterpret_cast<const double2 *>(v4 + 4 * (size_t)row);
+    const double hi = v4[4 * (size_t)row + 2];
+    return V3{ lo.x, lo.y, hi };
+}
+
+/* L2-only loads for data other CTAs write during the kernel (z, p, partials): never
+ * served from this SM's L1, so correctness does not depend on L1 invalidation. */
+__device__ __forceinline__ V3 ldcg3(const double *v4, int row) {
+    const double2 lo = __ldcg(reinterpret_cast<const double2 *>(v4 + 4 * (size_t)row));
+    const double hi = __ldcg(v4 + 4 * (size_t)row + 2);
+    return V3{ lo.x, lo.y, hi };
+}
+
+/* read-only (non-coherent path) variant for data no CTA writes during the kernel */
+__device__ __forceinline__ V3 ldg3(const double *v4, int row) {
+    const double2 lo = __ldg(reinterpret_cast<const double2 *>(v4 + 4 * (size_t)row));
+    const double hi = __ldg(v4 + 4 * (size_t)row + 2);
+    return V3{ lo.x, lo.y, hi };
+}
+
+__device__ __forceinline__ void st3(double *v4, int row, V3 v) {
+    *reinterpret_cast<double2 *>(v4 + 4 * (size_t)row) = make_double2(v.a, v.b);
+    v4[4 * (size_t)row + 2] = v.c;
+}
+
+/* p_new = z + beta * p_old exactly as MatrixOps.c:382 (first iteration: p = z). */
+__device__ __forceinline__ V3 p_of(const double *z4, const double *pold4, int row, double beta,
+                                   bool first) {
+    V3 z = ldcg3(z4, row);
+    if (first) return z;
+    V3 p = ldcg3(pold4, row);
+    return V3{ z.a + beta * p.a, z.b + beta * p.b, z.c + beta * p.c };
+}
+
+/* z = D^-1 r: z_i = ((0 + d_i0 r0) + d_i1 r1) + d_i2 r2 (MatrixOps.c:369-377). */
+__device__ __forceinline__ V3 apply_dinv(const double *dinv, int row, V3 r) {
+    const double *d = dinv + 288 * (size_t)(row >> 5) + (row & 31);
+    double z0 = 0.0, z1 = 0.0, z2 = 0.0;
+    z0 = z0 + __ldg(d + 0) * r.a;   z0 = z0 + __ldg(d + 32) * r.b;  z0 = z0 + __ldg(d + 64) * r.c;
+    z1 = z1 + __ldg(d + 96) * r.a;  z1 = z1 + __ldg(d + 128) * r.b; z1 = z1 + __ldg(d + 160) * r.c;
+    z2 = z2 + __ldg(d + 192) * r.a; z2 = z2 + __ldg(d + 224) * r.b; z2 = z2 + __ldg(d + 256) * r.c;
+    return V3{ z0, z1, z2 };
+}
+
+/* q += block (3x3, slot layout at v) * p, each scalar row in column order. */
+__device__ __forceinline__ void blk_acc(const double *v, V3 p, double &q0, double &q1, double &q2) {
+    q0 = q0 + __ldg(v + 0) * p.a;   q0 = q0 + __ldg(v + 32) * p.b;  q0 = q0 + __ldg(v + 64) * p.c;
+    q1 = q1 + __ldg(v + 96) * p.a;  q1 = q1 + __ldg(v + 128) * p.b; q1 = q1 + __ldg(v + 160) * p.c;
+    q2 = q2 + __ldg(v + 192) * p.a; q2 = q2 + __ldg(v + 224) * p.b; q2 = q2 + __ldg(v + 256) * p.c;
+}
+
+/* Same as blk_acc for values that may live in shared or global memory. */
+__device__ __forceinline__ void blk_acc_any(const double *v, V3 p, double &q0, double &q1, double &q2) {
+    q0 = q0 + v[0] * p.a;   q0 = q0 + v[32] * p.b;  q0 = q0 + v[64] * p.c;
+    q1 = q1 + v[96] * p.a;  q1 = q1 + v[128] * p.b; q1 = q1 + v[160] * p.c;
+    q2 = q2 + v[192] * p.a; q2 = q2 + v[224] * p.b; q2 = q2 + v[256] * p.c;
+}
+
+#endif

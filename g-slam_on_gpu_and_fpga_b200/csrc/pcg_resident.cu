@@ -1,0 +1,249 @@
+/*
+ * pcg_resident.cu — the block-Jacobi PCG solver with the matrix resident in
+ * shared memory (reference algorithm: src/cpu_pcg_fp64/MatrixOps.c:281-391).
+ *
+ * The solver's matrix does not change during a solve, and at the sizes this
+ * back-end targets it fits in the GPU's aggregate shared memory (148 SMs x
+ * 227 KB): N = 100,000 poses is ~211 KB of FP64 blocks per SM. So each CTA of a
+ * cooperative launch (one per SM) copies its contiguous, slot-balanced share of
+ * the sliced matrix into shared memory once, with one TMA bulk copy
+ * (cp.async.bulk, completion on an mbarrier), and every PCG iteration after that
+ * reads values and column indices from shared memory. A share that does not fit
+ * reads its tail blocks from global memory (L2) instead.
+ *
+ * Each thread owns one block row for the whole solve and keeps that row's x, r,
+ * z and p in registers. Only what other rows need crosses L2 each iteration:
+ * p (published in phase A) and z (published in phase B), gathered by the rows
+ * that have a block in that column. Phases and reductions are those of pcg.cu:
+ *   A: p = z + beta p; q = A p (neighbours' p recomputed from their z and old p,
+ *      bit-identically); partial p.q                      -> grid reduction
+ *   B: x += alpha p; r -= alpha q; z = D^-1 r; partial r.r, r.z -> grid reduction
+ * Summation orders are unchanged: each scalar row of q adds its blocks in
+ * ascending original column order with separate multiply and add.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "gslam.h"
+#include "kernels.cuh"
+#include "pcg_common.cuh"
+
+/* ---- TMA bulk copy global -> shared, completion counted on an mbarrier ---- */
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+/* 16-byte aligned addresses, size a multiple of 16 (checked by the caller's layout). */
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src, unsigned bytes, uint64_t *bar) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+        "l"(src), "r"(bytes), "r"(b)
+        : "memory");
+}
+
+/* Waits for the staged copy with a time limit; false if it did not complete. */
+__device__ __forceinline__ bool wait_staged(uint64_t *bar, long long limit) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, 0)) {
+        if (clock64() - t0 > limit) return false;
+    }
+    return true;
+}
+
+template <int BS>
+__global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ double s_red[3][BS / 32];
+    __shared__ double s_bc[4];
+    __shared__ int s_ok;
+    __shared__ __align__(8) uint64_t s_bar;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int epoch = 0;
+    if ((int)blockIdx.x == P.absent_cta) return; /* test hook, see pcg.cu */
+
+    const int s0 = __ldg(P.cta_slice + blockIdx.x), s1 = __ldg(P.cta_slice + blockIdx.x + 1);
+    const int64_t slot0 = __ldg(P.slice_ptr + s0), slot1 = __ldg(P.slice_ptr + s1);
+    const int64_t nval = 9 * (slot1 - slot0);
+    const int64_t nsm = nval < P.smem_val_cap ? nval : P.smem_val_cap; /* multiple of 288 */
+    double *sval = reinterpret_cast<double *>(smem);
+    int *scol = reinterpret_cast<int *>(smem + 8 * P.smem_val_cap);
+
+    /* ---- stage this CTA's matrix share ---- */
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar, 1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned vbytes = (unsigned)(8 * nsm), cbytes = (unsigned)(4 * (slot1 - slot0));
+        mbar_expect_tx(&s_bar, vbytes + cbytes);
+        if (vbytes) bulk_g2s(sval, P.val + 9 * slot0, vbytes, &s_bar);
+        if (cbytes) bulk_g2s(scol, P.col + slot0, cbytes, &s_bar);
+        int ok = wait_staged(&s_bar, P.spin_limit);
+        if (!ok) {
+            atomicExch(&P.gs->abort, 1);
+            wait_staged(&s_bar, P.spin_limit); /* let the copy finish before the CTA leaves */
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) {
+        if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
+        return;
+    }
+
+    /* ---- this thread's row ---- */
+    const int s = s0 + warp;
+    const bool own_slice = s < s1;
+    const int row = 32 * s + lane;
+    const bool mine = own_slice && row < P.n_rows;
+    const int len = mine ? __ldg(P.row_len + row) : 0;
+    const int64_t lslot = own_slice ? (__ldg(P.slice_ptr + s) - slot0) : 0; /* local slot of (j=0) */
+    const double *gval = P.val + 9 * slot0;  /* global copy of this CTA's share */
+    const int *cb = scol + lslot + lane;
+
+    V3 x = { 0.0, 0.0, 0.0 }, r = { 0.0, 0.0, 0.0 }, z = { 0.0, 0.0, 0.0 }, pn = { 0.0, 0.0, 0.0 };
+    double acc2[2] = { 0.0, 0.0 };
+    if (mine) {
+        r = ldg3(P.b4, row);
+        z = apply_dinv(P.dinv, row, r);
+        st3(P.z4, row, z);
+        acc2[0] = acc2[0] + r.a * z.a; acc2[0] = acc2[0] + r.b * z.b; acc2[0] = acc2[0] + r.c * z.c;
+        acc2[1] = acc2[1] + r.a * r.a; acc2[1] = acc2[1] + r.b * r.b; acc2[1] = acc2[1] + r.c * r.c;
+    }
+    if (!grid_allreduce<2, BS>(acc2, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
+        if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
+        return;
+    }
+    double rz = acc2[0];
+    const double bnorm = sqrt(acc2[1]);
+    const double tol = P.tol_rel * bnorm;
+    double beta = 0.0, rr = acc2[1];
+    int k = 0, reason = GSLAM_STOP_MAXIT;
+
+    while (true) {
+        if (k >= P.max_iter) { reason = GSLAM_STOP_MAXIT; break; }
+        const bool first = (k == 0);
+        double *pnew = (k & 1) ? P.p4b : P.p4a;
+        const double *pold = (k & 1) ? P.p4a : P.p4b;
+        /* ---- phase A ---- */
+        double pq[1] = { 0.0 };
+        V3 q = { 0.0, 0.0, 0.0 };
+        if (mine) {
+            pn = first ? z : V3{ z.a + beta * pn.a, z.b + beta * pn.b, z.c + beta * pn.c };
+            st3(pnew, row, pn);
+            double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+            int j = 0;
+            for (; j + 1 < len; j += 2) {
+                const int c0 = cb[32 * j], c1 = cb[32 * (j + 1)];
+                const V3 p0 = p_of(P.z4, pold, c0, beta, first);
+                const V3 p1 = p_of(P.z4, pold, c1, beta, first);
+                const int64_t o0 = 9 * lslot + 288 * j, o1 = o0 + 288;
+                blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
+                blk_acc_any(o1 + 288 <= nsm ? sval + o1 + lane : gval + o1 + lane, p1, q0, q1, q2);
+            }
+            if (j < len) {
+                const int c0 = cb[32 * j];
+                const V3 p0 = p_of(P.z4, pold, c0, beta, first);
+                const int64_t o0 = 9 * lslot + 288 * j;
+                blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
+            }
+            q = V3{ q0, q1, q2 };
+            pq[0] = pq[0] + pn.a * q.a; pq[0] = pq[0] + pn.b * q.b; pq[0] = pq[0] + pn.c * q.c;
+        }
+        if (!grid_allreduce<1, BS>(pq, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
+            reason = GSLAM_STOP_TIMEOUT;
+            break;
+        }
+        if (pq[0] == 0.0) { reason = GSLAM_STOP_PQ_ZERO; break; }
+        const double alpha = rz / pq[0];
+        /* ---- phase B ---- */
+        double rs[2] = { 0.0, 0.0 };
+        if (mine) {
+            x.a = x.a + alpha * pn.a; x.b = x.b + alpha * pn.b; x.c = x.c + alpha * pn.c;
+            r.a = r.a - alpha * q.a;  r.b = r.b - alpha * q.b;  r.c = r.c - alpha * q.c;
+            rs[0] = rs[0] + r.a * r.a; rs[0] = rs[0] + r.b * r.b; rs[0] = rs[0] + r.c * r.c;
+            z = apply_dinv(P.dinv, row, r);
+            st3(P.z4, row, z);
+            rs[1] = rs[1] + r.a * z.a; rs[1] = rs[1] + r.b * z.b; rs[1] = rs[1] + r.c * z.c;
+        }
+        if (!grid_allreduce<2, BS>(rs, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
+            reason = GSLAM_STOP_TIMEOUT;
+            break;
+        }
+        k++;
+        rr = rs[0];
+        if (sqrt(rr) < tol) { reason = GSLAM_STOP_TOL; break; }
+        beta = rs[1] / rz;
+        rz = rs[1];
+    }
+    if (mine) st3(P.x4, row, x);
+    if (reason == GSLAM_STOP_TIMEOUT && threadIdx.x == 0) {
+        P.res->timeout = 1;
+        P.res->reason = GSLAM_STOP_TIMEOUT;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && reason != GSLAM_STOP_TIMEOUT) {
+        P.res->iterations = k;
+        P.res->reason = reason;
+        P.res->refinements = 0;
+        P.res->timeout = 0;
+        P.res->rnorm = sqrt(rr);
+        P.res->bnorm = bnorm;
+    }
+}
+
+/* 768 threads (24 slices per CTA, up to 85 registers) when the slices fit, else 1024;
+ * the host's slice partition uses the same cap (one slice per warp). */
+template <int BS>
+static cudaError_t set_smem_attr() {
+    return cudaFuncSetAttribute((const void *)k_pcg64_res<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                GSLAM_RES_SMEM_MAX);
+}
+
+cudaError_t launch_pcg_resident(cudaStream_t st, const PcgParams &p, int grid, int block,
+                                size_t smem_bytes) {
+    if (block != 768 && block != 1024) return cudaErrorInvalidValue;
+    /* the attribute is per function and process: set once (pcg_resident_max_grid sets it
+     * before any layout chooses this solver) */
+    PcgParams copy = p;
+    void *args[] = { &copy };
+    const void *fn = block == 768 ? (const void *)k_pcg64_res<768> : (const void *)k_pcg64_res<1024>;
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, smem_bytes, st);
+}
+
+int pcg_resident_max_grid(int device, size_t smem_bytes) {
+    int n_sm = 0, a = 0, b = 0;
+    if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (set_smem_attr<768>() != cudaSuccess || set_smem_attr<1024>() != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (const void *)k_pcg64_res<768>, 768, smem_bytes) !=
+        cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void *)k_pcg64_res<1024>, 1024, smem_bytes) !=
+        cudaSuccess)
+        return 0;
+    return std::min(a, b) * n_sm;
+}

@@ -21,6 +21,8 @@ class RoundStats:
     reason: int
     rel_residual: float
     diff: float
+    solve_ms: float = 0.0
+    round_ms: float = 0.0
 
 
 @dataclass
@@ -175,7 +177,14 @@ class PoseGraph:
     def round(self) -> RoundStats:
         st = abi.SolveStats()
         abi.check(abi.lib().gslam_round(self._h, C.byref(st)))
-        return RoundStats(st.iterations, st.refinements, st.reason, st.rel_residual, st.diff)
+        return RoundStats(st.iterations, st.refinements, st.reason, st.rel_residual, st.diff, st.solve_ms,
+                          st.round_ms)
+
+    def stream(self) -> int:
+        """The cudaStream_t (as an int) all work on this graph runs on."""
+        s = C.c_void_p()
+        abi.check(abi.lib().gslam_get_stream(self._h, C.byref(s)))
+        return s.value or 0
 
     def run(self, max_rounds: int):
         diffs = np.zeros(max(max_rounds, 1))
@@ -195,7 +204,7 @@ class PoseGraph:
     def solve(self) -> RoundStats:
         st = abi.SolveStats()
         abi.check(abi.lib().gslam_solve(self._h, C.byref(st)))
-        return RoundStats(st.iterations, st.refinements, st.reason, st.rel_residual, st.diff)
+        return RoundStats(st.iterations, st.refinements, st.reason, st.rel_residual, st.diff, st.solve_ms)
 
     def update(self) -> float:
         d = C.c_double()
@@ -234,7 +243,13 @@ class PoseGraph:
         """y = Omega x on device pointers (3N doubles each, original order)."""
         abi.check(abi.lib().gslam_spmv(self._h, C.c_void_p(d_x), C.c_void_p(d_y)))
 
-    def spmv_bench(self, fp32: bool, reps: int) -> float:
+    def spmv_bench(self, fp32: bool, reps: int, n_copies: int = 1) -> float:
+        """Mean device ms per SpMV over `reps` graph-replayed launches (see gslam.h)."""
         ms = C.c_float()
-        abi.check(abi.lib().gslam_spmv_bench(self._h, int(fp32), int(reps), C.byref(ms)))
+        abi.check(abi.lib().gslam_spmv_bench(self._h, int(fp32), int(reps), int(n_copies), C.byref(ms)))
         return ms.value
+
+    def spmv_bytes(self, fp32: bool) -> int:
+        b = C.c_int64()
+        abi.check(abi.lib().gslam_spmv_bytes(self._h, int(fp32), C.byref(b)))
+        return b.value

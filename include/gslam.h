@@ -61,6 +61,7 @@ typedef struct gslam_opts {
     double barrier_timeout_ms; /* a solver barrier gives up after this long; 0 = 2000 ms */
     int test_absent_cta;  /* test hook: this solver CTA never arrives at its first barrier, so
                              the others time out (checks the bounded wait); -1 = off */
+    int disable_resident; /* 1: never stage the matrix in shared memory (streamed solver only) */
 } gslam_opts;
 
 typedef struct gslam_solve_stats {
@@ -69,6 +70,8 @@ typedef struct gslam_solve_stats {
     int reason;           /* GSLAM_STOP_* */
     double rel_residual;  /* ||b - A x|| / ||b|| as tracked by the solver */
     double diff;          /* ||dx|| / sqrt(dim) (GSLAM.c:104-105) */
+    double solve_ms;      /* device time of the solver launch (CUDA events on the graph's stream) */
+    double round_ms;      /* gslam_round only: device time of the whole round */
 } gslam_solve_stats;
 
 /* Inputs of the reference's factor family, as read_data produces them (GSLAM.c:415-493). */
@@ -116,6 +119,9 @@ int gslam_set_opts(gslam_graph *g, const gslam_opts *opts);
 int gslam_sizes(const gslam_graph *g, int64_t *n_poses, int64_t *n_edges, int64_t *nnzb,
                 int64_t *nnz);
 
+/* The CUDA stream (cudaStream_t) every call on this graph runs on. */
+int gslam_get_stream(gslam_graph *g, void **stream);
+
 /* Pose state (x, y, theta per pose, original order). */
 int gslam_set_poses(gslam_graph *g, const double *poses);
 int gslam_get_poses(gslam_graph *g, double *poses);
@@ -154,8 +160,15 @@ int gslam_get_diag_inv(gslam_graph *g, double *dinv);
 
 /* y = Omega x on device pointers in original order [3N] (FP64, row sums in column order). */
 int gslam_spmv(gslam_graph *g, const double *d_x, double *d_y);
-/* Runs `reps` FP64 (prec 0) or FP32 (prec 1) SpMVs on the resident matrix; *ms = mean ms each. */
-int gslam_spmv_bench(gslam_graph *g, int prec, int reps, float *ms);
+/*
+ * Times `reps` FP64 (prec 0) or FP32 (prec 1) SpMVs y = Omega x, replayed from one CUDA
+ * graph; *ms = mean device milliseconds per SpMV. n_copies > 1 rotates through that many
+ * copies of the matrix values (allocated for the call) so consecutive SpMVs read different
+ * memory: with n_copies * bytes above three L2 sizes every SpMV streams from HBM.
+ */
+int gslam_spmv_bench(gslam_graph *g, int prec, int reps, int n_copies, float *ms);
+/* Algorithmic bytes of one SpMV: values, column indices, x read once, y written once. */
+int gslam_spmv_bytes(gslam_graph *g, int prec, int64_t *bytes);
 
 /* ---- host-only utilities (no GPU needed) ---- */
 /* Observation-edge order of make_edges (src/cpu_pcg_fp64/GSLAM.c:222-318): pairs of z-list
