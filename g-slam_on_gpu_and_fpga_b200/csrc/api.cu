@@ -171,11 +171,14 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
     L->grid = std::max(1, std::min(grid, needed));
     L->n_sm = n_sm;
     L->partial_capacity = std::max(L->grid, maxg);
-    /* resident solver: contiguous slice ranges per CTA balanced by slot count, at most
-     * one slice per warp (32 per CTA); values staged in shared memory up to its size */
+    /* resident solvers: contiguous slice ranges per CTA balanced by slot count, at most
+     * one slice per warp; the FP64 solver stages FP64 values, the mixed solver FP32
+     * values plus its own rows' D^-1 and halo, each up to the shared-memory budget */
     L->resident = false;
-    const int rgrid = pcg_resident_max_grid(device, GSLAM_RES_SMEM_MAX);
-    if (!o.disable_resident && rgrid > 0 && S.n_slices <= 32 * rgrid) {
+    L->mixed_ok = false;
+    const int rgrid = std::min(pcg_resident_max_grid(device, GSLAM_RES_SMEM_MAX),
+                               pcg_mixed_max_grid(device, GSLAM_RES_SMEM_MAX));
+    if (rgrid > 0 && S.n_slices <= 32 * rgrid) {
         const int block = (S.n_slices <= 24 * rgrid) ? 768 : 1024;
         const int cap_sl = block / 32;          /* one slice per warp */
         /* boundaries at equal shares of the slot prefix sum, then clamped so that no
@@ -199,16 +202,29 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             if (cs[i + 1] < cs[i] || cs[i + 1] - cs[i] > cap_sl) ok = false;
             max_slots = std::max(max_slots, S.slice_ptr[cs[i + 1]] - S.slice_ptr[cs[i]]);
         }
-        const int64_t col_bytes = (4 * max_slots + 127) / 128 * 128;
-        const int64_t cap = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes) / 8 / 288 * 288;
-        if (ok && cap >= 0) {
-            L->resident = true;
+        if (ok) {
             L->res_grid = rgrid;
             L->res_block = block;
-            L->smem_val_cap = std::min<int64_t>(cap, 9 * max_slots);
-            L->smem_bytes = (size_t)(8 * L->smem_val_cap + 4 * max_slots);
             CK(dupload(m, st, &L->cta_slice, cs));
             L->partial_capacity = std::max(L->partial_capacity, rgrid);
+            const int64_t col_bytes = (4 * max_slots + 127) / 128 * 128;
+            /* FP64: values | columns */
+            const int64_t cap64 = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes) / 8 / 288 * 288;
+            if (cap64 >= 0 && !o.disable_resident) {
+                L->resident = true;
+                L->smem_val_cap = std::min<int64_t>(cap64, 9 * max_slots);
+                L->smem_bytes = (size_t)(8 * L->smem_val_cap + 4 * max_slots);
+            }
+            /* mixed: FP32 values | columns | D^-1 of own rows (2304 B per slice) | halo */
+            const int64_t fixed = col_bytes + 2304 * (int64_t)cap_sl + 36 * 32 * (int64_t)cap_sl;
+            const int64_t cap32 = ((int64_t)GSLAM_RES_SMEM_MAX - fixed) / 4 / 288 * 288;
+            if (cap32 >= 0) {
+                L->mixed_ok = true;
+                L->mixed_val_cap = std::min<int64_t>(cap32, 9 * max_slots);
+                L->mixed_dinv_off = 4 * L->mixed_val_cap + col_bytes;
+                L->mixed_halo_off = L->mixed_dinv_off + 2304 * (int64_t)cap_sl;
+                L->mixed_smem_bytes = (size_t)(L->mixed_halo_off + 36 * 32 * (int64_t)cap_sl);
+            }
         }
     }
     CK(dalloc(m, &L->partials, 8 * (size_t)L->partial_capacity));
@@ -274,21 +290,29 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
     P.absent_cta = o.test_absent_cta;
     CK(cudaMemsetAsync(L->gs, 0, sizeof(GridSync), st));
     CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
-    const bool resident = L->resident && fused_prec == GSLAM_PREC_FP64 && !o.disable_resident;
-    const int grid = resident ? L->res_grid : L->grid;
+    const bool mixed = fused_prec == GSLAM_PREC_MIXED;
+    if (mixed && !L->mixed_ok) {
+        g_last_error = "mixed precision needs the graph's rows to fit the resident layout (<= 32 slices per SM)";
+        return GSLAM_ERR_TOO_LARGE;
+    }
+    const bool resident = !mixed && L->resident && !o.disable_resident;
+    const int grid = (resident || mixed) ? L->res_grid : L->grid;
     {
         /* 2 barriers per iteration + 1: the arrival counter must not wrap */
-        const double barriers = 2.0 * (double)std::max(o.max_iter, 0) + 4.0;
+        const double barriers = 2.0 * (double)std::max(o.max_iter, 0) + 4.0 * (double)std::max(o.max_refine, 1) + 4.0;
         if (barriers * (double)grid >= 4294967295.0) {
             g_last_error = "max_iter too large for the solver's 32-bit barrier counter";
             return GSLAM_ERR_TOO_LARGE;
         }
     }
     P.cta_slice = L->cta_slice;
-    P.smem_val_cap = L->smem_val_cap;
+    P.smem_val_cap = mixed ? L->mixed_val_cap : L->smem_val_cap;
+    P.smem_dinv_off = L->mixed_dinv_off;
+    P.smem_halo_off = L->mixed_halo_off;
     tr.step("memsets");
     CK(cudaEventRecord(L->ev0, st));
-    if (resident) CK(launch_pcg_resident(st, P, grid, L->res_block, L->smem_bytes));
+    if (mixed) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->mixed_smem_bytes));
+    else if (resident) CK(launch_pcg_resident(st, P, grid, L->res_block, L->smem_bytes));
     else CK(launch_pcg(st, P, fused_prec, grid, L->block));
     tr.step("solver launch");
     CK(cudaEventRecord(L->ev1, st));

@@ -76,6 +76,8 @@ struct PcgParams {
     int absent_cta;        /* test hook: CTA that leaves before its first barrier, -1 = none */
     const int *cta_slice;  /* resident solver: [grid + 1] first slice of each CTA */
     int64_t smem_val_cap;  /* resident solver: values (multiple of 288) staged in shared memory */
+    int64_t smem_dinv_off; /* mixed solver: byte offsets of own-row D^-1 and halo in shared memory */
+    int64_t smem_halo_off;
 };
 
 /* Cooperative launch of the persistent solver; returns the CUDA error. */
@@ -87,6 +89,10 @@ int pcg_max_grid(int precision, int block, int device);
 cudaError_t launch_pcg_resident(cudaStream_t st, const PcgParams &p, int grid, int block,
                                 size_t smem_bytes);
 int pcg_resident_max_grid(int device, size_t smem_bytes);
+
+/* Mixed-precision solver (pcg_mixed.cu). */
+cudaError_t launch_pcg_mixed(cudaStream_t st, const PcgParams &p, int grid, int block, size_t smem_bytes);
+int pcg_mixed_max_grid(int device, size_t smem_bytes);
 
 /* Standalone SpMV y = A x on padded new-order vectors (FP64 or FP32 values). */
 void launch_spmv64(cudaStream_t st, int n_rows, int n_slices, const int64_t *slice_ptr,

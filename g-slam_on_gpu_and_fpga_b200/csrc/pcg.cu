@@ -41,29 +41,6 @@
 /* ------------------------------------------------------------------------ */
 
 /*
- * One row of q = A p with p formed on the fly from z and the previous p. Two
- * blocks per step so both columns' gathers are in flight together; blocks are
- * still added in ascending column order.
- */
-__device__ __forceinline__ V3 spmv_row(const double *vb, const int *cb, int len, const double *z4,
-                                       const double *pold, double beta, bool first) {
-    double q0 = 0.0, q1 = 0.0, q2 = 0.0;
-    int j = 0;
-    for (; j + 1 < len; j += 2) {
-        const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
-        const V3 p0 = p_of(z4, pold, c0, beta, first);
-        const V3 p1 = p_of(z4, pold, c1, beta, first);
-        blk_acc(vb + 288 * j, p0, q0, q1, q2);
-        blk_acc(vb + 288 * (j + 1), p1, q0, q1, q2);
-    }
-    if (j < len) {
-        const int c0 = __ldg(cb + 32 * j);
-        blk_acc(vb + 288 * j, p_of(z4, pold, c0, beta, first), q0, q1, q2);
-    }
-    return V3{ q0, q1, q2 };
-}
-
-/*
  * ONE: every warp owns at most one slice, so a row's p and q stay in registers
  * from phase A to phase B; otherwise they go through memory.
  */

@@ -29,50 +29,7 @@
 #include "gslam.h"
 #include "kernels.cuh"
 #include "pcg_common.cuh"
-
-/* ---- TMA bulk copy global -> shared, completion counted on an mbarrier ---- */
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-/* 16-byte aligned addresses, size a multiple of 16 (checked by the caller's layout). */
-__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src, unsigned bytes, uint64_t *bar) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
-        "l"(src), "r"(bytes), "r"(b)
-        : "memory");
-}
-
-/* Waits for the staged copy with a time limit; false if it did not complete. */
-__device__ __forceinline__ bool wait_staged(uint64_t *bar, long long limit) {
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, 0)) {
-        if (clock64() - t0 > limit) return false;
-    }
-    return true;
-}
+#include "tma_bulk.cuh"
 
 template <int BS>
 __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
@@ -94,19 +51,19 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
 
     /* ---- stage this CTA's matrix share ---- */
     if (threadIdx.x == 0) {
-        mbar_init(&s_bar, 1);
+        tma_mbar_init(&s_bar, 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned vbytes = (unsigned)(8 * nsm), cbytes = (unsigned)(4 * (slot1 - slot0));
-        mbar_expect_tx(&s_bar, vbytes + cbytes);
-        if (vbytes) bulk_g2s(sval, P.val + 9 * slot0, vbytes, &s_bar);
-        if (cbytes) bulk_g2s(scol, P.col + slot0, cbytes, &s_bar);
-        int ok = wait_staged(&s_bar, P.spin_limit);
+        tma_mbar_expect_tx(&s_bar, vbytes + cbytes);
+        if (vbytes) tma_bulk_g2s(sval, P.val + 9 * slot0, vbytes, &s_bar);
+        if (cbytes) tma_bulk_g2s(scol, P.col + slot0, cbytes, &s_bar);
+        int ok = tma_wait(&s_bar, 0, P.spin_limit);
         if (!ok) {
             atomicExch(&P.gs->abort, 1);
-            wait_staged(&s_bar, P.spin_limit); /* let the copy finish before the CTA leaves */
+            tma_wait(&s_bar, 0, P.spin_limit); /* let the copy finish before the CTA leaves */
         }
         s_ok = ok;
     }
@@ -158,17 +115,18 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
             st3(pnew, row, pn);
             double q0 = 0.0, q1 = 0.0, q2 = 0.0;
             int j = 0;
+            /* the diagonal block's column is this row: its p is already in registers */
             for (; j + 1 < len; j += 2) {
                 const int c0 = cb[32 * j], c1 = cb[32 * (j + 1)];
-                const V3 p0 = p_of(P.z4, pold, c0, beta, first);
-                const V3 p1 = p_of(P.z4, pold, c1, beta, first);
+                const V3 p0 = c0 == row ? pn : p_of(P.z4, pold, c0, beta, first);
+                const V3 p1 = c1 == row ? pn : p_of(P.z4, pold, c1, beta, first);
                 const int64_t o0 = 9 * lslot + 288 * j, o1 = o0 + 288;
                 blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
                 blk_acc_any(o1 + 288 <= nsm ? sval + o1 + lane : gval + o1 + lane, p1, q0, q1, q2);
             }
             if (j < len) {
                 const int c0 = cb[32 * j];
-                const V3 p0 = p_of(P.z4, pold, c0, beta, first);
+                const V3 p0 = c0 == row ? pn : p_of(P.z4, pold, c0, beta, first);
                 const int64_t o0 = 9 * lslot + 288 * j;
                 blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
             }
