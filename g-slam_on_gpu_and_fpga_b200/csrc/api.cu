@@ -256,6 +256,10 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
     if (fused_prec == GSLAM_PREC_MIXED) {
         int rc = gslam_layout_ensure_fp32(L, st);
         if (rc != GSLAM_OK) return rc;
+        if (!L->val32_fresh) {
+            launch_val_to_f32(st, 9 * L->n_slots, L->val, L->val32);
+            L->val32_fresh = true;
+        }
     }
     HostTrace tr;
     launch_diag_inv(st, L->n_rows, L->diag_slot, L->val, L->dinv);
@@ -565,6 +569,7 @@ int gslam_assemble_ex(gslam_graph *g, const double *blocks, double *csr_vals, do
     }
     launch_assemble(g->st, g->L.n_slots, g->d_ctr_ptr, g->d_ctr, blocks, g->S.anchor_slot, g->anchor,
                     g->L.val, v32, g->L.slot_csr, g->L.chunk_slice, g->L.row_len, csr_vals);
+    g->L.val32_fresh = (v32 != nullptr);
     launch_assemble_xi(g->st, g->n_poses, g->d_xi_ptr, g->d_xi_ctr, blocks, g->L.b4, g->L.perm,
                        xi_orig);
     CK(cudaGetLastError());

@@ -155,6 +155,7 @@ void device_pcg_solve(double *x_h, double *d_csr_vals, double *d_xi, int dim, in
     gslam_graph *g = s_graph;
     launch_csr_to_sell(g->st, g->L.n_slots, g->L.slot_csr, g->L.chunk_slice, g->L.row_len, d_csr_vals,
                        g->L.val, nullptr);
+    g->L.val32_fresh = false;
     launch_gather_vec(g->st, g->n_poses, g->L.perm, d_xi, g->L.b4);
     DCK(cudaGetLastError(), "device_pcg_solve");
     gslam_opts o = g->o;
@@ -275,6 +276,7 @@ void pcg_solve_sparse(double *x, CSRMatrix *csr, double *b, unsigned int dim) {
         for (int c = 0; c < 3; c++) C.hb[4 * (size_t)nr + c] = b[3 * (size_t)C.S.perm[nr] + c];
     DCK(cudaMemcpyAsync(C.L.val, C.hval.data(), C.hval.size() * sizeof(double), cudaMemcpyHostToDevice, C.st),
         "pcg_solve_sparse");
+    C.L.val32_fresh = false;
     DCK(cudaMemcpyAsync(C.L.b4, C.hb.data(), C.hb.size() * sizeof(double), cudaMemcpyHostToDevice, C.st),
         "pcg_solve_sparse");
     gslam_opts o;

@@ -27,6 +27,7 @@ struct DevLayout {
     int64_t *slice_ptr = nullptr, *slot_csr = nullptr;
     double *val = nullptr, *dinv = nullptr;
     float *val32 = nullptr;
+    bool val32_fresh = false;      /* val32 holds the current values */
     double *b4 = nullptr, *x4 = nullptr, *r4 = nullptr, *z4 = nullptr;
     double *p4a = nullptr, *p4b = nullptr, *q4 = nullptr;
     float *f[6] = { nullptr, nullptr, nullptr, nullptr, nullptr, nullptr };

@@ -185,6 +185,12 @@ __global__ void k_sell_to_csr(int64_t n_slots, const int64_t *__restrict__ slot_
     }
 }
 
+/* FP64 values -> FP32 copy (same layout), for a mixed solve of values assembled in FP64 mode. */
+__global__ void k_val_to_f32(int64_t n, const double *__restrict__ val, float *__restrict__ val32) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) val32[i] = (float)val[i];
+}
+
 /* Original-order vector [3N] -> padded new-order vector [4N]. */
 __global__ void k_gather_vec(int n_rows, const int *__restrict__ perm, const double *__restrict__ src,
                              double *__restrict__ dst4) {
@@ -344,6 +350,10 @@ void launch_csr_to_sell(cudaStream_t st, int64_t n_slots, const int64_t *slot_cs
                         double *val, float *val32) {
     k_csr_to_sell<<<blocks_for(9 * n_slots, 256), 256, 0, st>>>(n_slots, slot_csr, chunk_slice,
                                                                row_len, csr_vals, val, val32);
+}
+
+void launch_val_to_f32(cudaStream_t st, int64_t n, const double *val, float *val32) {
+    if (n > 0) k_val_to_f32<<<blocks_for(n, 256), 256, 0, st>>>(n, val, val32);
 }
 
 void launch_gather_vec(cudaStream_t st, int n_rows, const int *perm, const double *src, double *dst4) {

@@ -26,6 +26,7 @@ void launch_assemble_xi(cudaStream_t st, int n_rows, const int64_t *xi_ptr, cons
 void launch_csr_to_sell(cudaStream_t st, int64_t n_slots, const int64_t *slot_csr,
                         const int *chunk_slice, const int *row_len, const double *csr_vals,
                         double *val, float *val32);
+void launch_val_to_f32(cudaStream_t st, int64_t n, const double *val, float *val32);
 void launch_gather_vec(cudaStream_t st, int n_rows, const int *perm, const double *src, double *dst4);
 void launch_scatter_vec(cudaStream_t st, int n_rows, const int *perm, const double *src4, double *dst);
 void launch_diag_inv(cudaStream_t st, int n_rows, const int *diag_slot, const double *val,
