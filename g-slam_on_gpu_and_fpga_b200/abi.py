@@ -37,7 +37,7 @@ EXPORTS = [
     "gslam_version", "gslam_last_error", "gslam_obs_edge_order", "gslam_csr_pattern",
     "pcg_solve_sparse", "device_graph_init", "device_graph_update", "device_graph_get_row_ptr",
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
-    "gslam_dropin_status",
+    "gslam_dropin_status", "gslam_pcg_solve_static",
 ]
 
 
@@ -153,6 +153,8 @@ def lib() -> C.CDLL:
             "device_build_diag_inv": [C.c_int],
             "device_graph_free": [],
             "gslam_dropin_status": [],
+            "gslam_pcg_solve_static": [C.c_int, VP, VP, VP, VP, VP, C.c_double, C.c_int, VP,
+                                       C.POINTER(SolveStats)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

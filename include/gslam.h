@@ -198,6 +198,29 @@ typedef struct gslam_log {
 int gslam_read_log(const char *path, gslam_log **out);
 void gslam_free_log(gslam_log *log);
 
+/* ---- solve without any device allocation ---- */
+/*
+ * No counterpart in the reference. For callers that cannot allocate device memory when
+ * they solve: work being recorded into a CUDA graph, processes whose device memory is
+ * owned by another allocator or fixed up front, real-time loops. Solves the reference's
+ * system (scalar CSR of Omega, dim = 3 * poses, columns ascending within a row; all
+ * pointers are device memory the caller owns) with block-Jacobi PCG in FP64
+ * (||r|| < tol ||b|| or max_iter iterations, x overwritten) on `stream`
+ * (a cudaStream_t; NULL = legacy default stream), using a fixed scratch array inside the
+ * library: GSLAM_STATIC_SCRATCH_BYTES on every GPU that loads the library, held until
+ * the process exits; systems above GSLAM_STATIC_MAX_POSES poses return
+ * GSLAM_ERR_TOO_LARGE. It calls no cudaMalloc or cudaFree. The first call on a device
+ * looks up the scratch's device address and caches it: make that first call before any
+ * stream capture. All calls share the scratch, so calls that overlap on the GPU race:
+ * serialise them. stats (host, may be NULL) makes the call wait for the result;
+ * without it the call returns as soon as the solve is queued.
+ */
+#define GSLAM_STATIC_SCRATCH_BYTES (4u << 20)
+#define GSLAM_STATIC_MAX_POSES 16384
+int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *d_col_idx,
+                           const double *d_values, const double *d_b, double *d_x, double tol,
+                           int max_iter, void *stream, gslam_solve_stats *stats);
+
 /* Library version string and the error text of the last failing call on this thread. */
 const char *gslam_version(void);
 const char *gslam_last_error(void);
