@@ -12,6 +12,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -208,12 +209,41 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             CK(dupload(m, st, &L->cta_slice, cs));
             L->partial_capacity = std::max(L->partial_capacity, rgrid);
             const int64_t col_bytes = (4 * max_slots + 127) / 128 * 128;
-            /* FP64: values | columns */
-            const int64_t cap64 = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes) / 8 / 288 * 288;
+            /* CTA-local column indices (own rows first, then the CTA's halo) and halo lists */
+            std::vector<int> lcol(S.n_slots, 0), hptr(rgrid + 1, 0), hrows;
+            int64_t p_cap = 0;
+            for (int i = 0; i < rgrid; i++) {
+                const int row0 = 32 * cs[i], row1 = 32 * cs[i + 1], nloc = row1 - row0;
+                const int64_t a0 = S.slice_ptr[cs[i]], a1 = S.slice_ptr[cs[i + 1]];
+                std::vector<int> rem;
+                for (int64_t t = a0; t < a1; t++) {
+                    const int c = S.col[t];
+                    if (c >= 0 && (c < row0 || c >= row1)) rem.push_back(c);
+                }
+                std::sort(rem.begin(), rem.end());
+                rem.erase(std::unique(rem.begin(), rem.end()), rem.end());
+                for (int64_t t = a0; t < a1; t++) {
+                    const int c = S.col[t];
+                    if (c < 0) lcol[t] = 0;
+                    else if (c >= row0 && c < row1) lcol[t] = c - row0;
+                    else lcol[t] = nloc + (int)(std::lower_bound(rem.begin(), rem.end(), c) - rem.begin());
+                }
+                hptr[i + 1] = hptr[i] + (int)rem.size();
+                hrows.insert(hrows.end(), rem.begin(), rem.end());
+                p_cap = std::max<int64_t>(p_cap, nloc + (int64_t)rem.size());
+            }
+            /* FP64: values | local columns | staged p (32 B per own or halo row) */
+            const int64_t p_bytes = 32 * p_cap;
+            const int64_t cap64 = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes - p_bytes) / 8 / 288 * 288;
             if (cap64 >= 0 && !o.disable_resident) {
                 L->resident = true;
                 L->smem_val_cap = std::min<int64_t>(cap64, 9 * max_slots);
-                L->smem_bytes = (size_t)(8 * L->smem_val_cap + 4 * max_slots);
+                L->smem_p_off = 8 * L->smem_val_cap + col_bytes;
+                L->smem_bytes = (size_t)(L->smem_p_off + p_bytes);
+                CK(dupload(m, st, &L->lcol, lcol));
+                CK(dupload(m, st, &L->halo_ptr, hptr));
+                if (hrows.empty()) hrows.push_back(0);
+                CK(dupload(m, st, &L->halo_rows, hrows));
             }
             /* mixed: FP32 values | columns | D^-1 of own rows (2304 B per slice) | halo */
             const int64_t fixed = col_bytes + 2304 * (int64_t)cap_sl + 36 * 32 * (int64_t)cap_sl;
@@ -313,6 +343,10 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
     P.smem_val_cap = mixed ? L->mixed_val_cap : L->smem_val_cap;
     P.smem_dinv_off = L->mixed_dinv_off;
     P.smem_halo_off = L->mixed_halo_off;
+    P.lcol = L->lcol;
+    P.halo_ptr = L->halo_ptr;
+    P.halo_rows = L->halo_rows;
+    P.smem_p_off = L->smem_p_off;
     tr.step("memsets");
     CK(cudaEventRecord(L->ev0, st));
     if (mixed) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->mixed_smem_bytes));

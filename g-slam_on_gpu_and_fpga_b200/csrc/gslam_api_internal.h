@@ -42,6 +42,8 @@ struct DevLayout {
     int res_grid = 0, res_block = 0;
     int *cta_slice = nullptr;      /* [res_grid + 1] */
     int64_t smem_val_cap = 0;      /* doubles staged per CTA */
+    int *lcol = nullptr, *halo_ptr = nullptr, *halo_rows = nullptr; /* CTA-local columns, halo lists */
+    int64_t smem_p_off = 0;        /* staged p, after values and columns */
     size_t smem_bytes = 0;
     bool mixed_ok = false;          /* the mixed solver's shared-memory layout fits */
     int64_t mixed_val_cap = 0;     /* floats staged per CTA */

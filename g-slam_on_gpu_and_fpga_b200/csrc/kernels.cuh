@@ -79,6 +79,10 @@ struct PcgParams {
     int64_t smem_val_cap;  /* resident solver: values (multiple of 288) staged in shared memory */
     int64_t smem_dinv_off; /* mixed solver: byte offsets of own-row D^-1 and halo in shared memory */
     int64_t smem_halo_off;
+    const int *lcol;       /* resident solver: per slot, CTA-local column index (own rows, then halo) */
+    const int *halo_ptr;   /* resident solver: [grid + 1] halo list bounds per CTA */
+    const int *halo_rows;  /* resident solver: halo rows (new row indices) */
+    int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
 };
 
 /* Cooperative launch of the persistent solver; returns the CUDA error. */

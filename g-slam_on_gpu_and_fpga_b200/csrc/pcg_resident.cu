@@ -12,9 +12,13 @@
  * reads its tail blocks from global memory (L2) instead.
  *
  * Each thread owns one block row for the whole solve and keeps that row's x, r,
- * z and p in registers. Only what other rows need crosses L2 each iteration:
- * p (published in phase A) and z (published in phase B), gathered by the rows
- * that have a block in that column. Phases and reductions are those of pcg.cu:
+ * z and p in registers. Only what other CTAs need crosses L2 each iteration: p
+ * (phase A) and z (phase B). Column indices are staged as CTA-local indices: a
+ * CTA's own rows first, then its halo (the other CTAs' rows its blocks touch, a
+ * list fixed at setup). In phase A every owner writes its p to shared memory and
+ * all threads of the CTA together stage the halo's p from L2 in one parallel pass,
+ * so the SpMV reads values and p from shared memory only — one L2 round trip per
+ * phase instead of one per pair of blocks. Phases and reductions are those of pcg.cu:
  *   A: p = z + beta p; q = A p (neighbours' p recomputed from their z and old p,
  *      bit-identically); partial p.q                      -> grid reduction
  *   B: x += alpha p; r -= alpha q; z = D^-1 r; partial r.r, r.z -> grid reduction
@@ -47,7 +51,10 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     const int64_t nval = 9 * (slot1 - slot0);
     const int64_t nsm = nval < P.smem_val_cap ? nval : P.smem_val_cap; /* multiple of 288 */
     double *sval = reinterpret_cast<double *>(smem);
-    int *scol = reinterpret_cast<int *>(smem + 8 * P.smem_val_cap);
+    int *scol = reinterpret_cast<int *>(smem + 8 * P.smem_val_cap);   /* local column indices */
+    double *sp = reinterpret_cast<double *>(smem + P.smem_p_off);     /* p of own + halo rows */
+    const int n_loc = 32 * (s1 - s0), row0 = 32 * s0;
+    const int h0 = __ldg(P.halo_ptr + blockIdx.x), h1 = __ldg(P.halo_ptr + blockIdx.x + 1);
 
     /* ---- stage this CTA's matrix share ---- */
     if (threadIdx.x == 0) {
@@ -59,7 +66,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
         const unsigned vbytes = (unsigned)(8 * nsm), cbytes = (unsigned)(4 * (slot1 - slot0));
         tma_mbar_expect_tx(&s_bar, vbytes + cbytes);
         if (vbytes) tma_bulk_g2s(sval, P.val + 9 * slot0, vbytes, &s_bar);
-        if (cbytes) tma_bulk_g2s(scol, P.col + slot0, cbytes, &s_bar);
+        if (cbytes) tma_bulk_g2s(scol, P.lcol + slot0, cbytes, &s_bar);
         int ok = tma_wait(&s_bar, 0, P.spin_limit);
         if (!ok) {
             atomicExch(&P.gs->abort, 1);
@@ -107,26 +114,29 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
         const bool first = (k == 0);
         double *pnew = (k & 1) ? P.p4b : P.p4a;
         const double *pold = (k & 1) ? P.p4a : P.p4b;
-        /* ---- phase A ---- */
+        /* ---- phase A: p of own rows (registers -> shared + global for other CTAs),
+         *      p of halo rows staged from L2 by all threads, then q = A p from shared ---- */
         double pq[1] = { 0.0 };
         V3 q = { 0.0, 0.0, 0.0 };
         if (mine) {
             pn = first ? z : V3{ z.a + beta * pn.a, z.b + beta * pn.b, z.c + beta * pn.c };
             st3(pnew, row, pn);
+            st3(sp, row - row0, pn);
+        }
+        for (int h = h0 + (int)threadIdx.x; h < h1; h += BS)
+            st3(sp, n_loc + (h - h0), p_of(P.z4, pold, __ldg(P.halo_rows + h), beta, first));
+        __syncthreads();
+        if (mine) {
             double q0 = 0.0, q1 = 0.0, q2 = 0.0;
             int j = 0;
-            /* the diagonal block's column is this row: its p is already in registers */
             for (; j + 1 < len; j += 2) {
-                const int c0 = cb[32 * j], c1 = cb[32 * (j + 1)];
-                const V3 p0 = c0 == row ? pn : p_of(P.z4, pold, c0, beta, first);
-                const V3 p1 = c1 == row ? pn : p_of(P.z4, pold, c1, beta, first);
+                const V3 p0 = ld3(sp, cb[32 * j]), p1 = ld3(sp, cb[32 * (j + 1)]);
                 const int64_t o0 = 9 * lslot + 288 * j, o1 = o0 + 288;
                 blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
                 blk_acc_any(o1 + 288 <= nsm ? sval + o1 + lane : gval + o1 + lane, p1, q0, q1, q2);
             }
             if (j < len) {
-                const int c0 = cb[32 * j];
-                const V3 p0 = c0 == row ? pn : p_of(P.z4, pold, c0, beta, first);
+                const V3 p0 = ld3(sp, cb[32 * j]);
                 const int64_t o0 = 9 * lslot + 288 * j;
                 blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
             }
