@@ -223,8 +223,27 @@ def e2e_arm(G, torch, g, stream, steps):
     return total, 3 * n * 8, 3 * n * 8
 
 
+def pose_err_rel(p, ref):
+    """||p - ref|| / ||ref|| over all pose components, angle differences wrapped."""
+    import numpy as np
+    d = p - ref
+    d[:, 2] = (d[:, 2] + np.pi) % (2 * np.pi) - np.pi
+    return float(np.linalg.norm(d) / np.linalg.norm(ref))
+
+
+def poses_after(G, cg, precision, rounds):
+    g = G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=LAMBDA,
+                             tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=precision)
+    for _ in range(rounds):
+        g.round()
+    p = g.poses.copy()
+    g.close()
+    return p
+
+
 def cpu_baseline_sample(cg, rounds=2):
-    """The oracle (reference algorithm in C, one thread) on the same workload."""
+    """The oracle (reference algorithm in C, one thread) on the same workload; returns
+    rounds/s, the seconds taken and the poses after `rounds` rounds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
 
@@ -240,7 +259,7 @@ def cpu_baseline_sample(cg, rounds=2):
         poses = poses + dx.reshape(-1, 3)
         poses[:, 2] = (poses[:, 2] + np.pi) % (2 * np.pi) - np.pi
     dt = time.perf_counter() - t0
-    return rounds / dt, dt
+    return rounds / dt, dt, poses
 
 
 def run_ours(args):
@@ -255,7 +274,7 @@ def run_ours(args):
     peaks, peak_kind = measured_peaks()
 
     results = {}
-    for arm, prec in (("fp64", G.abi.PREC_FP64),):
+    for arm, prec in (("fp64", G.abi.PREC_FP64), ("mixed", G.abi.PREC_MIXED)):
         barrier(dist)
         torch.cuda.synchronize()
         with ClockSampler(local) as clk:
@@ -269,40 +288,63 @@ def run_ours(args):
         results[arm] = dict(g=g, sizes=sizes, rounds=rounds, solves=solves, iters=iters,
                             total_ms=total_ms, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h, clocks=clk.summary())
 
-    r = results["fp64"]
-    s_a = s_v = 8
-    nb, nnzb = r["sizes"]["n_poses"], r["sizes"]["nnzb"]
-    b_iter = pcg_bytes_per_iteration(nnzb, nb, s_a, s_v)
-    mean_iters = statistics.mean(r["iters"])
-    mean_solve_ms = statistics.mean(r["solves"])
-    achieved = b_iter * mean_iters / (mean_solve_ms * 1e-3) / 1e9
-    traffic_it = solver_traffic_per_iteration("fp64")
-    value = world * args.steps / (r["total_ms"] * 1e-3)
+    def arm_summary(r, s_a, s_v):
+        nb, nnzb = r["sizes"]["n_poses"], r["sizes"]["nnzb"]
+        b_iter = pcg_bytes_per_iteration(nnzb, nb, s_a, s_v)
+        mean_iters = statistics.mean(r["iters"])
+        mean_solve_ms = statistics.mean(r["solves"])
+        return dict(nnzb=nnzb, b_iter=b_iter, mean_iters=mean_iters, mean_solve_ms=mean_solve_ms,
+                    achieved=b_iter * mean_iters / (mean_solve_ms * 1e-3) / 1e9,
+                    value=world * args.steps / (r["total_ms"] * 1e-3),
+                    e2e=world * args.steps / (r["e2e_ms"] * 1e-3))
+
+    f, m = arm_summary(results["fp64"], 8, 8), arm_summary(results["mixed"], 4, 4)
+    # pose error after two rounds from the initial guess: against the CPU oracle (the
+    # reference's FP64 PCG) when it runs here, and against this library's FP64 solve
+    p_fp64 = poses_after(G, cg, G.abi.PREC_FP64, 2)
+    p_mixed = poses_after(G, cg, G.abi.PREC_MIXED, 2)
+    err = {"rounds": 2, "mixed_vs_gpu_fp64": pose_err_rel(p_mixed, p_fp64)}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt, p_oracle = cpu_baseline_sample(cg)
+        cpu = {"value": round(v, 5), "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"2 GN rounds of the same N=100000 workload ({dt:.1f} s)"}
+        err["mixed_vs_oracle"] = pose_err_rel(p_mixed, p_oracle)
+        err["gpu_fp64_vs_oracle"] = pose_err_rel(p_fp64, p_oracle)
+    traffic_it = solver_traffic_per_iteration("mixed")
+    r = results["mixed"]
     line = {
-        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "metric": METRIC, "value": round(m["value"], 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(r["total_ms"] / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded city-grid walk; no dataset)",
-        "config": config({"solver": "fp64 block-Jacobi PCG, matrix resident in shared memory",
-                          "nnzb": nnzb, "pcg_iterations_mean": mean_iters,
+        "dtype": "f32 inner / f64 refinement", "data": "synthetic (seeded city-grid walk; no dataset)",
+        "config": config({"solver": "mixed-precision PCG: FP32 inner Chronopoulos-Gear iterations, FP64 "
+                                    "residual / dots / D^-1 / pose accumulation (iterative refinement)",
+                          "nnzb": m["nnzb"], "pcg_iterations_mean": m["mean_iters"],
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
-        "roofline": {"kernel": "k_pcg64_res (persistent PCG solve)", "bound": "hbm",
-                     "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_iteration": b_iter,
-                     "traffic": (round(traffic_it * mean_iters) if traffic_it else None),
-                     "solve_ms_mean": round(mean_solve_ms, 4),
-                     "us_per_pcg_iteration": round(1e3 * mean_solve_ms / mean_iters, 3)},
-        "e2e": {"value": round(world * args.steps / (r["e2e_ms"] * 1e-3), 3), "unit": UNIT,
+        "fp64": {"value": round(f["value"], 3), "unit": UNIT,
+                 "ms_per_step": round(results["fp64"]["total_ms"] / args.steps, 4),
+                 "pcg_iterations_mean": f["mean_iters"],
+                 "us_per_pcg_iteration": round(1e3 * f["mean_solve_ms"] / f["mean_iters"], 3),
+                 "e2e": round(f["e2e"], 3), "achieved_gbs": round(f["achieved"], 1),
+                 "clocks": results["fp64"]["clocks"]},
+        "mixed_vs_fp64": round(m["value"] / f["value"], 3),
+        "pose_err_rel": err,
+        "roofline": {"kernel": "k_pcg_mixed (persistent mixed-precision solve)", "bound": "hbm",
+                     "achieved": round(m["achieved"], 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(m["achieved"] / peaks["hbm_gbs"], 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_iteration": m["b_iter"],
+                     "traffic": (round(traffic_it * m["mean_iters"]) if traffic_it else None),
+                     "solve_ms_mean": round(m["mean_solve_ms"], 4),
+                     "us_per_pcg_iteration": round(1e3 * m["mean_solve_ms"] / m["mean_iters"], 3)},
+        "e2e": {"value": round(m["e2e"], 3), "unit": UNIT,
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
         "gpu_launches": 7 * args.steps,
         "clocks": r["clocks"],
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, dt = cpu_baseline_sample(cg)
-        line["cpu_baseline"] = {"value": round(v, 5), "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": f"2 GN rounds of the same N=100000 workload ({dt:.1f} s)"}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     for arm in results.values():
         arm["g"].close()
     if rank == 0:

@@ -182,22 +182,39 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
     if (rgrid > 0 && S.n_slices <= 32 * rgrid) {
         const int block = (S.n_slices <= 24 * rgrid) ? 768 : 1024;
         const int cap_sl = block / 32;          /* one slice per warp */
-        /* boundaries at equal shares of the slot prefix sum, then clamped so that no
-         * CTA owns more than cap_sl slices (feasible since n_slices <= cap_sl * rgrid) */
-        std::vector<int> cs(rgrid + 1);
-        const int64_t total = S.n_slots;
-        int sl = 0;
-        for (int i = 0; i <= rgrid; i++) {
-            const int64_t want = total * i / rgrid;
-            while (sl < S.n_slices && S.slice_ptr[sl] < want) sl++;
-            cs[i] = sl;
+        /* contiguous slice ranges of at most cap_sl slices that minimise the largest
+         * slot count of any CTA (the slowest CTA sets the pace of every iteration):
+         * binary search on that bound, each probe a greedy fill; feasible at the
+         * upper end since n_slices <= cap_sl * rgrid */
+        auto fill = [&](int64_t bound, std::vector<int> *out) {
+            int used = 1, nsl = 0;
+            int64_t cur = 0;
+            if (out) (*out)[0] = 0;
+            for (int sl = 0; sl < S.n_slices; sl++) {
+                const int64_t w = S.slice_ptr[sl + 1] - S.slice_ptr[sl];
+                if (nsl > 0 && (cur + w > bound || nsl == cap_sl)) {
+                    if (out && used <= rgrid) (*out)[used] = sl;
+                    used++;
+                    cur = 0;
+                    nsl = 0;
+                }
+                cur += w;
+                nsl++;
+            }
+            if (out)
+                for (int i = std::min(used, rgrid); i <= rgrid; i++) (*out)[i] = S.n_slices;
+            return used;
+        };
+        int64_t lo = 0, hi = S.n_slots;
+        for (int sl = 0; sl < S.n_slices; sl++) lo = std::max(lo, S.slice_ptr[sl + 1] - S.slice_ptr[sl]);
+        while (lo < hi) {
+            const int64_t mid = lo + (hi - lo) / 2;
+            if (fill(mid, nullptr) <= rgrid) hi = mid;
+            else lo = mid + 1;
         }
-        cs[0] = 0;
-        cs[rgrid] = S.n_slices;
-        for (int i = 1; i <= rgrid; i++) cs[i] = std::min(std::max(cs[i], cs[i - 1]), cs[i - 1] + cap_sl);
-        cs[rgrid] = S.n_slices;
-        for (int i = rgrid - 1; i >= 0; i--) cs[i] = std::max(std::min(cs[i], cs[i + 1]), cs[i + 1] - cap_sl);
-        bool ok = cs[0] == 0;
+        std::vector<int> cs(rgrid + 1);
+        fill(lo, &cs);
+        bool ok = cs[0] == 0 && cs[rgrid] == S.n_slices;
         int64_t max_slots = 0;
         for (int i = 0; i < rgrid; i++) {
             if (cs[i + 1] < cs[i] || cs[i + 1] - cs[i] > cap_sl) ok = false;
@@ -212,6 +229,7 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             /* CTA-local column indices (own rows first, then the CTA's halo) and halo lists */
             std::vector<int> lcol(S.n_slots, 0), hptr(rgrid + 1, 0), hrows;
             int64_t p_cap = 0;
+            int sl_max = 0;
             for (int i = 0; i < rgrid; i++) {
                 const int row0 = 32 * cs[i], row1 = 32 * cs[i + 1], nloc = row1 - row0;
                 const int64_t a0 = S.slice_ptr[cs[i]], a1 = S.slice_ptr[cs[i + 1]];
@@ -231,6 +249,7 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 hptr[i + 1] = hptr[i] + (int)rem.size();
                 hrows.insert(hrows.end(), rem.begin(), rem.end());
                 p_cap = std::max<int64_t>(p_cap, nloc + (int64_t)rem.size());
+                sl_max = std::max(sl_max, cs[i + 1] - cs[i]);
             }
             /* FP64: values | local columns | staged p (32 B per own or halo row) */
             const int64_t p_bytes = 32 * p_cap;
@@ -240,20 +259,24 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 L->smem_val_cap = std::min<int64_t>(cap64, 9 * max_slots);
                 L->smem_p_off = 8 * L->smem_val_cap + col_bytes;
                 L->smem_bytes = (size_t)(L->smem_p_off + p_bytes);
-                CK(dupload(m, st, &L->lcol, lcol));
-                CK(dupload(m, st, &L->halo_ptr, hptr));
-                if (hrows.empty()) hrows.push_back(0);
-                CK(dupload(m, st, &L->halo_rows, hrows));
             }
-            /* mixed: FP32 values | columns | D^-1 of own rows (2304 B per slice) | halo */
-            const int64_t fixed = col_bytes + 2304 * (int64_t)cap_sl + 36 * 32 * (int64_t)cap_sl;
+            /* mixed: FP32 values | local columns | D^-1 of own rows (2304 B per slice) |
+             * z of own and halo rows (16 B each) */
+            const int64_t z_bytes = (16 * p_cap + 127) / 128 * 128;
+            const int64_t fixed = col_bytes + 2304 * (int64_t)sl_max + z_bytes;
             const int64_t cap32 = ((int64_t)GSLAM_RES_SMEM_MAX - fixed) / 4 / 288 * 288;
             if (cap32 >= 0) {
                 L->mixed_ok = true;
                 L->mixed_val_cap = std::min<int64_t>(cap32, 9 * max_slots);
                 L->mixed_dinv_off = 4 * L->mixed_val_cap + col_bytes;
-                L->mixed_halo_off = L->mixed_dinv_off + 2304 * (int64_t)cap_sl;
-                L->mixed_smem_bytes = (size_t)(L->mixed_halo_off + 36 * 32 * (int64_t)cap_sl);
+                L->mixed_halo_off = L->mixed_dinv_off + 2304 * (int64_t)sl_max;
+                L->mixed_smem_bytes = (size_t)(L->mixed_halo_off + z_bytes);
+            }
+            if (L->resident || L->mixed_ok) {
+                CK(dupload(m, st, &L->lcol, lcol));
+                CK(dupload(m, st, &L->halo_ptr, hptr));
+                if (hrows.empty()) hrows.push_back(0);
+                CK(dupload(m, st, &L->halo_rows, hrows));
             }
         }
     }

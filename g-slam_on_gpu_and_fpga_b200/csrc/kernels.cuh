@@ -77,7 +77,7 @@ struct PcgParams {
     int absent_cta;        /* test hook: CTA that leaves before its first barrier, -1 = none */
     const int *cta_slice;  /* resident solver: [grid + 1] first slice of each CTA */
     int64_t smem_val_cap;  /* resident solver: values (multiple of 288) staged in shared memory */
-    int64_t smem_dinv_off; /* mixed solver: byte offsets of own-row D^-1 and halo in shared memory */
+    int64_t smem_dinv_off; /* mixed solver: byte offsets of own-row D^-1 and of z (own + halo rows) */
     int64_t smem_halo_off;
     const int *lcol;       /* resident solver: per slot, CTA-local column index (own rows, then halo) */
     const int *halo_ptr;   /* resident solver: [grid + 1] halo list bounds per CTA */

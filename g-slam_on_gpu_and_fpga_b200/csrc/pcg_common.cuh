@@ -68,16 +68,28 @@ __device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned epoch, long 
 }
 
 /*
- * Deterministic all-reduce of NV doubles across the grid. v[] holds this
- * thread's partials on entry and the grid totals on exit.
+ * Deterministic all-reduce of NV (<= 4) doubles across the grid, in pieces so that
+ * a caller can issue loads of data the other CTAs published before the barrier
+ * while the partials are summed, and can derive scalars from the totals in one
+ * thread instead of all of them:
+ *   grid_reduce_arrive:  block sum of each thread's v[], one partial per CTA,
+ *                        grid barrier (false: the solve must be abandoned);
+ *   grid_reduce_sum:     warp i < NV sums the CTAs' partials of value i into
+ *                        s_bc[i] (a lane's loads all in flight together, a fixed
+ *                        order: lane-strided, then a shuffle tree), then a
+ *                        barrier among those NV warps, so thread 0 sees every total;
+ *   grid_reduce_collect: grid_reduce_sum, CTA barrier, v[] = the totals everywhere.
+ * Two partial buffers alternate: a CTA can be at most one reduction ahead of the
+ * slowest reader, so it never overwrites partials still being summed.
  */
+#define GSLAM_SUM_UNROLL 5 /* partial loads per lane issued together (grids up to 160 CTAs) */
+
 template <int NV, int BS>
-__device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials_base, int &epoch,
-                                               GridSync *gs, long long spin_limit,
-                                               double (*s_red)[BS / 32], double *s_bc, int *s_ok) {
+__device__ __forceinline__ bool grid_reduce_arrive(const double (&v)[NV], double *partials_base, int &epoch,
+                                                   GridSync *gs, long long spin_limit,
+                                                   double (*s_red)[BS / 32], int *s_ok) {
+    static_assert(NV <= 4 && BS / 32 <= 32, "reduction shape");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    /* Two partial buffers alternate: a CTA can be at most one reduction ahead of
-     * the slowest reader, so it never overwrites partials still being summed. */
     double *partials = partials_base + (epoch & 1) * 4 * gridDim.x;
     epoch++;                                   /* this reduction's barrier number */
 #pragma unroll
@@ -88,26 +100,52 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials
         if (lane == 0) s_red[i][warp] = a;
     }
     __syncthreads();
-    if (threadIdx.x < NV) {
-        double s = 0.0;
+    if (warp < NV) {
+        double a = lane < BS / 32 ? s_red[warp][lane] : 0.0;
 #pragma unroll
-        for (int w = 0; w < BS / 32; w++) s = s + s_red[threadIdx.x][w];
-        partials[threadIdx.x * gridDim.x + blockIdx.x] = s;
+        for (int o = 16; o > 0; o >>= 1) a = a + __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) partials[warp * gridDim.x + blockIdx.x] = a;
     }
-    if (!grid_barrier(gs, (unsigned)epoch, spin_limit, s_ok)) return false;
-    if (warp == 0) {
+    return grid_barrier(gs, (unsigned)epoch, spin_limit, s_ok);
+}
+
+template <int NV>
+__device__ __forceinline__ void grid_reduce_sum(const double *partials_base, int epoch, double *s_bc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp >= NV) return;
+    const int G = (int)gridDim.x;
+    const double *pp = partials_base + ((epoch - 1) & 1) * 4 * G + warp * G;
+    double t[GSLAM_SUM_UNROLL];
 #pragma unroll
-        for (int i = 0; i < NV; i++) {
-            double s = 0.0;
-            for (int c = lane; c < (int)gridDim.x; c += 32) s = s + __ldcg(partials + i * gridDim.x + c);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) s_bc[i] = s;
-        }
+    for (int u = 0; u < GSLAM_SUM_UNROLL; u++) {
+        const int c = lane + 32 * u;
+        t[u] = c < G ? __ldcg(pp + c) : 0.0;
     }
+    double s = t[0];
+#pragma unroll
+    for (int u = 1; u < GSLAM_SUM_UNROLL; u++) s = s + t[u];
+    for (int c = lane + 32 * GSLAM_SUM_UNROLL; c < G; c += 32) s = s + __ldcg(pp + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) s_bc[warp] = s;
+    if (NV > 1) asm volatile("bar.sync 1, %0;" ::"r"(NV * 32) : "memory");
+}
+
+template <int NV, int BS>
+__device__ __forceinline__ void grid_reduce_collect(double (&v)[NV], const double *partials_base, int epoch,
+                                                    double *s_bc) {
+    grid_reduce_sum<NV>(partials_base, epoch, s_bc);
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < NV; i++) v[i] = s_bc[i];
+}
+
+template <int NV, int BS>
+__device__ __forceinline__ bool grid_allreduce(double (&v)[NV], double *partials_base, int &epoch,
+                                               GridSync *gs, long long spin_limit,
+                                               double (*s_red)[BS / 32], double *s_bc, int *s_ok) {
+    if (!grid_reduce_arrive<NV, BS>(v, partials_base, epoch, gs, spin_limit, s_red, s_ok)) return false;
+    grid_reduce_collect<NV, BS>(v, partials_base, epoch, s_bc);
     return true;
 }
 

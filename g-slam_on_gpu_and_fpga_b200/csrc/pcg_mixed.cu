@@ -5,26 +5,40 @@
  * Precisions (the reference solves everything in FP64: MatrixOps.c:281-391):
  *   FP64: the outer residual r = xi - Omega x (FP64 matrix), the solution x, every
  *         global dot product (accumulated in FP64), the 3x3 block inverses D^-1
- *         (applied in FP64 and rounded to FP32).
- *   FP32: the inner SpMV (FP32 copy of Omega, staged in shared memory) and the
- *         inner vector updates.
+ *         (stored and applied in FP64, the product rounded to FP32).
+ *   FP32: the inner SpMV (FP32 copy of Omega, staged in shared memory), the inner
+ *         vector updates and the inner correction d (x += d in FP64 after each
+ *         inner solve).
  *
- * Inner iteration (Chronopoulos & Gear 1989, "s-step" CG with s = 1): with
- * s = A p and w = A z carried as recurrences, alpha and beta come from ONE fused
- * reduction of (r.z, w.z, r.r) per iteration instead of the two of standard PCG:
- *     x += alpha_{k-1} p_{k-1};  r_k = r_{k-1} - alpha_{k-1} s_{k-1};  z_k = D^-1 r_k
- *     w_k = A z_k;  gamma = r.z, delta = w.z, rho = r.r            -> grid reduction
+ * Inner iteration (Chronopoulos & Gear 1989, "s-step" CG with s = 1, in the
+ * preconditioned form that also carries M^-1 of the recurrence vectors): with
+ * s = A p, w = A z, u = M^-1 w and v = M^-1 s, alpha and beta come from ONE
+ * fused reduction of (r.z, w.z, r.r) per iteration instead of the two of
+ * standard PCG (M = the block diagonal, M^-1 = D^-1):
+ *     s_{k-1} = w_{k-1} + beta s_{k-2};   v_{k-1} = u_{k-1} + beta v_{k-2}
+ *     r_k = r_{k-1} - alpha s_{k-1};      z_k = z_{k-1} - alpha v_{k-1}
+ *     p_{k-1} = z_{k-1} + beta p_{k-2};   d += alpha p_{k-1}
+ *     w_k = A z_k;  u_k = D^-1 w_k;  gamma = r.z, delta = w.z, rho = r.r  -> reduction
  *     beta_k = gamma_k / gamma_{k-1};  alpha_k = gamma_k / (delta_k - beta_k gamma_k / alpha_{k-1})
- *     p_k = z_k + beta_k p_{k-1};  s_k = w_k + beta_k s_{k-1}
- * The SpMV needs z_k of neighbouring rows, which are only final after their own
- * r update; instead of a second grid barrier each row publishes r_k, w_k and
- * s_{k-1} before the reduction, and a neighbour's z_k is recomputed from those
- * (s_{k-1} = w_{k-1} + beta s_{k-2}, r_k = r_{k-1} - alpha s_{k-1}, z_k = D^-1 r_k)
- * with the same device function the owner uses, so it is bit-identical. Rows owned
- * by the same CTA read those values and D^-1 from shared memory; others from L2.
+ * (alpha, beta = those of the previous reduction). The SpMV needs z_k of rows
+ * other CTAs own, which is only final after the reduction; instead of a second
+ * grid barrier every row publishes (z_k, u_k, v_{k-1}) before the reduction and
+ * a reader forms v_k and z_{k+1} from them with the same two FP32 FMAs per
+ * component the owner uses, so the copies are bit-identical and no reader needs
+ * the owner's D^-1.
  *
- * Outer step: publish x (FP64), grid barrier, r = xi - Omega x with the FP64
- * matrix, ||r|| -> stop at tol * ||xi||, else restart the inner solve from r.
+ * Shared memory holds, per CTA: its FP32 matrix share, CTA-local column indices
+ * (own rows first, then the CTA's halo: the other CTAs' rows its blocks touch, a
+ * list fixed at setup), its own rows' D^-1, and z of its own and halo rows. Each
+ * thread owns one row and keeps r, z, s, v, w, u, p, d in registers; every thread
+ * also advances z of (at least) one halo row per iteration. The halo's published
+ * values are loaded right after the grid barrier, while warps 0-2 sum the
+ * reduction partials, so the two L2 round trips overlap; thread 0 alone then
+ * advances the scalar recurrence. The SpMV reads values, columns and z from
+ * shared memory only.
+ *
+ * Outer step: x += d (FP64), grid barrier, r = xi - Omega x with the FP64 matrix,
+ * ||r|| -> stop at tol * ||xi||, else restart the inner solve from r.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -43,27 +57,35 @@ __device__ __forceinline__ F3 ldcgf3(const float *v4, int row) {
     return F3{ v.x, v.y, v.z };
 }
 
+__device__ __forceinline__ F3 ldf3(const float *v4, int row) {
+    const float4 v = *reinterpret_cast<const float4 *>(v4 + 4 * (size_t)row);
+    return F3{ v.x, v.y, v.z };
+}
+
 __device__ __forceinline__ void stf3(float *v4, int row, F3 v) {
     *reinterpret_cast<float4 *>(v4 + 4 * (size_t)row) = make_float4(v.a, v.b, v.c, 0.f);
 }
 
-/* z = D^-1 r in FP64 (dinv rows at stride 32), rounded to FP32. */
-__device__ __forceinline__ F3 dinv_apply_f(const double *d, F3 r) {
-    const double r0 = r.a, r1 = r.b, r2 = r.c;
-    double z0 = 0.0, z1 = 0.0, z2 = 0.0;
-    z0 = z0 + d[0] * r0;   z0 = z0 + d[32] * r1;  z0 = z0 + d[64] * r2;
-    z1 = z1 + d[96] * r0;  z1 = z1 + d[128] * r1; z1 = z1 + d[160] * r2;
-    z2 = z2 + d[192] * r0; z2 = z2 + d[224] * r1; z2 = z2 + d[256] * r2;
-    return F3{ (float)z0, (float)z1, (float)z2 };
+/* y = D^-1 x in FP64 (the 9 entries of D^-1 at stride 32 doubles), rounded to FP32. */
+__device__ __forceinline__ F3 dinv_apply_f(const double *d, F3 x) {
+    const double x0 = x.a, x1 = x.b, x2 = x.c;
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    y0 = y0 + d[0] * x0;   y0 = y0 + d[32] * x1;  y0 = y0 + d[64] * x2;
+    y1 = y1 + d[96] * x0;  y1 = y1 + d[128] * x1; y1 = y1 + d[160] * x2;
+    y2 = y2 + d[192] * x0; y2 = y2 + d[224] * x1; y2 = y2 + d[256] * x2;
+    return F3{ (float)y0, (float)y1, (float)y2 };
 }
 
-/* The shared recurrence step: from (r_{k-1}, w_{k-1}, s_{k-2}) to (s_{k-1}, r_k). */
-__device__ __forceinline__ void step_rs(F3 r_old, F3 w_old, F3 s_old2, float alpha, float beta,
-                                        F3 &s_new, F3 &r_new) {
-    s_new = F3{ __fmaf_rn(beta, s_old2.a, w_old.a), __fmaf_rn(beta, s_old2.b, w_old.b),
-                __fmaf_rn(beta, s_old2.c, w_old.c) };
-    r_new = F3{ __fmaf_rn(-alpha, s_new.a, r_old.a), __fmaf_rn(-alpha, s_new.b, r_old.b),
-                __fmaf_rn(-alpha, s_new.c, r_old.c) };
+/* a * x + y, one FP32 FMA per component: every inner vector update */
+__device__ __forceinline__ F3 axpy_f(float a, F3 x, F3 y) {
+    return F3{ __fmaf_rn(a, x.a, y.a), __fmaf_rn(a, x.b, y.b), __fmaf_rn(a, x.c, y.c) };
+}
+
+/* v = u + beta v_old; z = z_old - alpha v: the step every copy of a row's z takes */
+__device__ __forceinline__ void step_zv(F3 z_old, F3 u, F3 v_old, float alpha, float beta, F3 &z_new,
+                                        F3 &v_new) {
+    v_new = axpy_f(beta, v_old, u);
+    z_new = axpy_f(-alpha, v_new, z_old);
 }
 
 __device__ __forceinline__ void blk_acc_f(const float *v, F3 p, float &q0, float &q1, float &q2) {
@@ -72,9 +94,6 @@ __device__ __forceinline__ void blk_acc_f(const float *v, F3 p, float &q0, float
     q2 = __fmaf_rn(v[192], p.a, q2); q2 = __fmaf_rn(v[224], p.b, q2); q2 = __fmaf_rn(v[256], p.c, q2);
 }
 
-/* halo record of one row in shared memory: r, w, s (FP32) */
-struct Halo { float r[3], w[3], s[3]; };
-
 template <int BS>
 __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -82,20 +101,26 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     __shared__ double s_bc[4];
     __shared__ int s_ok;
     __shared__ __align__(8) uint64_t s_bar;
+    /* scalar recurrence, kept and advanced by thread 0 only (no registers in the
+     * other threads): gamma_{k-1}, alpha_{k-1}, rho_0 of the inner solve, tol */
+    __shared__ double s_sc[4];
+    __shared__ float s_ab[2];  /* alpha, beta for the next iteration */
+    __shared__ int s_flag;     /* 0 continue, 1 inner solve done, 2 breakdown */
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int epoch = 0;
     if ((int)blockIdx.x == P.absent_cta) return; /* test hook, see pcg.cu */
 
     const int s0 = __ldg(P.cta_slice + blockIdx.x), s1 = __ldg(P.cta_slice + blockIdx.x + 1);
-    const int row0 = 32 * s0, row1 = 32 * s1;
+    const int row0 = 32 * s0, n_loc = 32 * (s1 - s0);
     const int64_t slot0 = __ldg(P.slice_ptr + s0), slot1 = __ldg(P.slice_ptr + s1);
     const int64_t nval = 9 * (slot1 - slot0);
     const int64_t nsm = nval < P.smem_val_cap ? nval : P.smem_val_cap;
-    /* dynamic shared memory: FP32 values | columns | D^-1 of own rows | halo of own rows */
+    const int h0 = __ldg(P.halo_ptr + blockIdx.x), h1 = __ldg(P.halo_ptr + blockIdx.x + 1);
+    /* dynamic shared memory: FP32 values | local columns | D^-1 of own rows | z of own + halo rows */
     float *sval = reinterpret_cast<float *>(smem);
     int *scol = reinterpret_cast<int *>(smem + 4 * P.smem_val_cap);
     double *sdinv = reinterpret_cast<double *>(smem + P.smem_dinv_off);
-    Halo *shalo = reinterpret_cast<Halo *>(smem + P.smem_halo_off);
+    float *sz = reinterpret_cast<float *>(smem + P.smem_halo_off);
 
     if (threadIdx.x == 0) {
         tma_mbar_init(&s_bar, 1);
@@ -107,7 +132,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
         const unsigned dbytes = (unsigned)(2304 * (s1 - s0));
         tma_mbar_expect_tx(&s_bar, vbytes + cbytes + dbytes);
         if (vbytes) tma_bulk_g2s(sval, P.val32 + 9 * slot0, vbytes, &s_bar);
-        if (cbytes) tma_bulk_g2s(scol, P.col + slot0, cbytes, &s_bar);
+        if (cbytes) tma_bulk_g2s(scol, P.lcol + slot0, cbytes, &s_bar);
         if (dbytes) tma_bulk_g2s(sdinv, P.dinv + 288 * (size_t)s0, dbytes, &s_bar);
         int ok = tma_wait(&s_bar, 0, P.spin_limit);
         if (!ok) {
@@ -127,23 +152,26 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     const int row = 32 * s + lane;
     const bool mine = own_slice && row < P.n_rows;
     const int len = mine ? __ldg(P.row_len + row) : 0;
-    const int64_t lslot = own_slice ? (__ldg(P.slice_ptr + s) - slot0) : 0;
-    const float *gval = P.val32 + 9 * slot0;
-    const int *cb = scol + lslot + lane;
-    const double *my_d = sdinv + 288 * (size_t)warp + lane; /* own row's D^-1 (stride 32) */
-    Halo *my_h = shalo + (row - row0);
+    /* 32-bit offsets into this CTA's share: local slot of (j = 0), and how many of the
+     * row's blocks have their values in shared memory (the rest are read from L2) */
+    const int lslot = own_slice ? (int)(__ldg(P.slice_ptr + s) - slot0) : 0;
+    const int j_sm = min(len, max(0, ((int)nsm - 9 * lslot) / 288));
+    /* the halo row this thread advances every iteration (more, in a loop, only when
+     * the halo has more rows than the CTA has threads) */
+    const int hh = h0 + (int)threadIdx.x;
+    const bool has_h = hh < h1;
+    const int hrow = has_h ? __ldg(P.halo_rows + hh) : 0;
 
-    /* published halo in global memory, double-buffered by iteration parity */
-    /* (selected by parity with ?: so no local-memory array is needed) */
-#define HALO_R(par) ((par) ? P.rf4 : P.xf4)
-#define HALO_W(par) ((par) ? P.pfa4 : P.zf4)
-#define HALO_S(par) ((par) ? P.qf4 : P.pfb4)
+    /* published (z_k, u_k, v_{k-1}) in global memory, double-buffered by iteration
+     * parity (selected with ?: so no local-memory array is needed) */
+#define PUB_Z(par) ((par) ? P.rf4 : P.xf4)
+#define PUB_U(par) ((par) ? P.pfa4 : P.zf4)
+#define PUB_V(par) ((par) ? P.qf4 : P.pfb4)
 
     /* ---- ||xi|| ---- */
     double bb[1] = { 0.0 };
-    V3 b = { 0.0, 0.0, 0.0 };
     if (mine) {
-        b = ldg3(P.b4, row);
+        const V3 b = ldg3(P.b4, row);
         bb[0] = bb[0] + b.a * b.a; bb[0] = bb[0] + b.b * b.b; bb[0] = bb[0] + b.c * b.c;
     }
     if (!grid_allreduce<1, BS>(bb, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
@@ -151,127 +179,131 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
         return;
     }
     const double bnorm = sqrt(bb[0]);
-    const double tol = P.tol_rel * bnorm;
+    if (threadIdx.x == 0) s_sc[3] = P.tol_rel * bnorm;
 
-    V3 x = { 0.0, 0.0, 0.0 };   /* FP64 solution */
-    V3 r64 = b;                 /* FP64 residual, = b for x = 0 */
+    V3 x = { 0.0, 0.0, 0.0 };   /* FP64 solution (P.x4 holds it during an inner solve) */
+    V3 r64 = mine ? ldg3(P.b4, row) : V3{ 0.0, 0.0, 0.0 }; /* FP64 residual, = xi for x = 0 */
     double rnorm = bnorm;
     int total = 0, outer = 0, reason = GSLAM_STOP_MAXIT;
     bool timed_out = false;
 
     while (true) {
-        if (rnorm < tol) { reason = GSLAM_STOP_TOL; break; }
+        if (rnorm < P.tol_rel * bnorm) { reason = GSLAM_STOP_TOL; break; }
         if (total >= P.max_iter || outer >= P.max_refine) { reason = GSLAM_STOP_MAXIT; break; }
         outer++;
-        /* ---- inner FP32 solve of A d = r64, accumulated into x ---- */
+        /* ---- inner FP32 solve of A d = r64; x += d in FP64 afterwards ---- */
+        if (mine) st3(P.x4, row, x);  /* x is not held in registers during the inner solve */
         F3 r = { (float)r64.a, (float)r64.b, (float)r64.c };
-        F3 z = { 0.f, 0.f, 0.f }, w = { 0.f, 0.f, 0.f }, sv = { 0.f, 0.f, 0.f }, p = { 0.f, 0.f, 0.f };
-        /* state "k = -1": r_{-1} = r0, w_{-1} = 0, s_{-2} = 0, alpha = beta = 0 */
+        const F3 zero = { 0.f, 0.f, 0.f };
+        /* state "k = -1": z_{-1} = D^-1 r_0, and w, u, s, v, p of earlier steps 0, so
+         * with alpha = beta = 0 the first step leaves r and z unchanged; readers of
+         * iteration 0 use parity (0 - 1) & 1 = 1 */
+        F3 z = mine ? dinv_apply_f(sdinv + 288 * warp + lane, r) : zero;
+        F3 w = zero, u = zero, sv = zero, v = zero, p = zero, d = zero;
         if (mine) {
-            const int par = 1; /* readers of iteration 0 use parity (0 - 1) & 1 = 1 */
-            stf3(HALO_R(par), row, r);
-            stf3(HALO_W(par), row, F3{ 0.f, 0.f, 0.f });
-            stf3(HALO_S(par), row, F3{ 0.f, 0.f, 0.f });
-            my_h->r[0] = r.a; my_h->r[1] = r.b; my_h->r[2] = r.c;
-            my_h->w[0] = my_h->w[1] = my_h->w[2] = 0.f;
-            my_h->s[0] = my_h->s[1] = my_h->s[2] = 0.f;
+            stf3(PUB_Z(1), row, z);
+            stf3(PUB_U(1), row, zero);
+            stf3(PUB_V(1), row, zero);
         }
         if (!grid_barrier(P.gs, (unsigned)(++epoch), P.spin_limit, &s_ok)) { timed_out = true; break; }
+        F3 hz = zero, hu = zero, hv = zero;
+        if (has_h) { hz = ldcgf3(PUB_Z(1), hrow); hu = ldcgf3(PUB_U(1), hrow); hv = ldcgf3(PUB_V(1), hrow); }
         float alpha = 0.f, beta = 0.f;
-        double gamma_prev = 1.0, alpha_prev = 1.0, rho0 = -1.0;
         int k = 0;
         while (true) {
             const int pr = (k - 1) & 1, pw = k & 1;
-            /* own recurrence, identical to what neighbours compute from the halo */
-            F3 s_new, r_new;
-            step_rs(r, w, sv, alpha, beta, s_new, r_new);
-            /* x += alpha p_{k-1} (FP64), p_{k-1} = z_{k-1} + beta p_{k-2} */
-            const F3 p_new = { __fmaf_rn(beta, p.a, z.a), __fmaf_rn(beta, p.b, z.b), __fmaf_rn(beta, p.c, z.c) };
-            if (k > 0) {
-                x.a = x.a + (double)alpha * (double)p_new.a;
-                x.b = x.b + (double)alpha * (double)p_new.b;
-                x.c = x.c + (double)alpha * (double)p_new.c;
+            /* z_k of the halo rows (first: frees the prefetched registers) */
+            if (has_h) {
+                F3 zn, vn;
+                step_zv(hz, hu, hv, alpha, beta, zn, vn);
+                stf3(sz, n_loc + (int)threadIdx.x, zn);
             }
-            p = p_new;
-            sv = s_new;       /* s_{k-1} */
-            r = r_new;        /* r_k */
-            z = mine ? dinv_apply_f(my_d, r) : F3{ 0.f, 0.f, 0.f };
-            /* w_k = A z_k */
+            for (int h = hh + BS; h < h1; h += BS) {
+                const int c = __ldg(P.halo_rows + h);
+                F3 zn, vn;
+                step_zv(ldcgf3(PUB_Z(pr), c), ldcgf3(PUB_U(pr), c), ldcgf3(PUB_V(pr), c), alpha, beta, zn, vn);
+                stf3(sz, n_loc + (h - h0), zn);
+            }
+            /* own row: s_{k-1}, r_k, p_{k-1}, d, then v_{k-1}, z_k */
+            sv = axpy_f(beta, sv, w);
+            r = axpy_f(-alpha, sv, r);
+            p = axpy_f(beta, p, z);
+            if (k > 0) d = axpy_f(alpha, p, d);
+            step_zv(z, u, v, alpha, beta, z, v);
+            if (mine) stf3(sz, row - row0, z);
+            __syncthreads();
+            /* w_k = A z_k from shared memory, u_k = D^-1 w_k */
             double part[3] = { 0.0, 0.0, 0.0 };
             if (mine) {
                 float q0 = 0.f, q1 = 0.f, q2 = 0.f;
-                for (int j = 0; j < len; j++) {
-                    const int c = cb[32 * j];
-                    F3 zc;
-                    if (c == row) {
-                        zc = z;
-                    } else if (c >= row0 && c < row1) {
-                        const Halo *h = shalo + (c - row0);
-                        F3 sn, rn;
-                        step_rs(F3{ h->r[0], h->r[1], h->r[2] }, F3{ h->w[0], h->w[1], h->w[2] },
-                                F3{ h->s[0], h->s[1], h->s[2] }, alpha, beta, sn, rn);
-                        const int cl = c - row0;
-                        zc = dinv_apply_f(sdinv + 288 * (size_t)(cl >> 5) + (cl & 31), rn);
-                    } else {
-                        F3 sn, rn;
-                        step_rs(ldcgf3(HALO_R(pr), c), ldcgf3(HALO_W(pr), c), ldcgf3(HALO_S(pr), c), alpha, beta,
-                                sn, rn);
-                        zc = dinv_apply_f(P.dinv + 288 * (size_t)(c >> 5) + (c & 31), rn);
-                    }
-                    const int64_t o = 9 * lslot + 288 * j;
-                    blk_acc_f(o + 288 <= nsm ? sval + o + lane : gval + o + lane, zc, q0, q1, q2);
-                }
+                const int *cb = scol + lslot + lane;
+                int j = 0;
+                for (; j < j_sm; j++)
+                    blk_acc_f(sval + 9 * lslot + 288 * j + lane, ldf3(sz, cb[32 * j]), q0, q1, q2);
+                for (; j < len; j++)
+                    blk_acc_f(P.val32 + 9 * (slot0 + lslot) + 288 * j + lane, ldf3(sz, cb[32 * j]), q0, q1, q2);
                 w = F3{ q0, q1, q2 };
+                u = dinv_apply_f(sdinv + 288 * warp + lane, w); /* own row's D^-1 (stride 32) */
                 const double r0 = r.a, r1 = r.b, r2 = r.c, z0 = z.a, z1 = z.b, z2 = z.c;
                 part[0] = r0 * z0 + r1 * z1 + r2 * z2;                            /* gamma */
                 part[1] = (double)w.a * z0 + (double)w.b * z1 + (double)w.c * z2; /* delta */
                 part[2] = r0 * r0 + r1 * r1 + r2 * r2;                            /* rho */
+                /* publish z_k, u_k, v_{k-1} for iteration k + 1 */
+                stf3(PUB_Z(pw), row, z);
+                stf3(PUB_U(pw), row, u);
+                stf3(PUB_V(pw), row, v);
             }
-            /* publish r_k, w_k, s_{k-1} for iteration k + 1 */
-            __syncthreads(); /* every local read of the previous halo is done */
-            if (mine) {
-                stf3(HALO_R(pw), row, r);
-                stf3(HALO_W(pw), row, w);
-                stf3(HALO_S(pw), row, sv);
-                my_h->r[0] = r.a; my_h->r[1] = r.b; my_h->r[2] = r.c;
-                my_h->w[0] = w.a; my_h->w[1] = w.b; my_h->w[2] = w.c;
-                my_h->s[0] = sv.a; my_h->s[1] = sv.b; my_h->s[2] = sv.c;
-            }
-            if (!grid_allreduce<3, BS>(part, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
+            if (!grid_reduce_arrive<3, BS>(part, P.partials, epoch, P.gs, P.spin_limit, s_red, &s_ok)) {
                 timed_out = true;
                 break;
             }
+            /* the halo's values for iteration k + 1, in flight while the partials are summed */
+            if (has_h) { hz = ldcgf3(PUB_Z(pw), hrow); hu = ldcgf3(PUB_U(pw), hrow); hv = ldcgf3(PUB_V(pw), hrow); }
+            grid_reduce_sum<3>(P.partials, epoch, s_bc);
             total++;
             k++;
-            const double gamma = part[0], delta = part[1], rho = part[2];
-            if (rho0 < 0.0) rho0 = rho;
-            double a, bt;
-            if (k == 1) { bt = 0.0; a = gamma / delta; }
-            else { bt = gamma / gamma_prev; a = gamma / (delta - bt * gamma / alpha_prev); }
-            if (!(delta != 0.0) || !(a == a)) { reason = GSLAM_STOP_PQ_ZERO; break; }
-            gamma_prev = gamma;
-            alpha_prev = a;
-            alpha = (float)a;
-            beta = (float)bt;
-            const bool inner_done = rho <= P.inner_tol * P.inner_tol * rho0 || k >= P.inner_max_iter ||
-                                    total >= P.max_iter || sqrt(rho) < tol;
-            if (inner_done) {
-                /* the last update: x += alpha_k p_k */
-                const F3 pf = { __fmaf_rn(beta, p.a, z.a), __fmaf_rn(beta, p.b, z.b), __fmaf_rn(beta, p.c, z.c) };
-                x.a = x.a + (double)alpha * (double)pf.a;
-                x.b = x.b + (double)alpha * (double)pf.b;
-                x.c = x.c + (double)alpha * (double)pf.c;
+            if (threadIdx.x == 0) {
+                const double gamma = s_bc[0], delta = s_bc[1], rho = s_bc[2];
+                if (k == 1) s_sc[2] = rho;
+                double a, bt;
+                if (k == 1) { bt = 0.0; a = gamma / delta; }
+                else { bt = gamma / s_sc[0]; a = gamma / (delta - bt * gamma / s_sc[1]); }
+                int flag = 0;
+                if (!(delta != 0.0) || !(a == a)) flag = 2;
+                else if (rho <= P.inner_tol * P.inner_tol * s_sc[2] || k >= P.inner_max_iter ||
+                         total >= P.max_iter || sqrt(rho) < s_sc[3])
+                    flag = 1;
+                s_sc[0] = gamma;
+                s_sc[1] = a;
+                s_ab[0] = (float)a;
+                s_ab[1] = (float)bt;
+                s_flag = flag;
+            }
+            __syncthreads();
+            const int flag = s_flag;
+            if (flag == 2) { reason = GSLAM_STOP_PQ_ZERO; break; }
+            alpha = s_ab[0];
+            beta = s_ab[1];
+            if (flag == 1) {
+                /* the last update: d += alpha_k p_k, p_k = z_k + beta_k p_{k-1} */
+                p = axpy_f(beta, p, z);
+                d = axpy_f(alpha, p, d);
                 break;
             }
         }
         if (timed_out) break;
-        /* ---- outer FP64 residual r64 = b - A x ---- */
-        if (mine) st3(P.x4, row, x);
+        /* ---- x += d in FP64, then the outer FP64 residual r64 = xi - A x ---- */
+        if (mine) {
+            x = ld3(P.x4, row);
+            x = V3{ x.a + (double)d.a, x.b + (double)d.b, x.c + (double)d.c };
+            st3(P.x4, row, x);
+        }
         if (!grid_barrier(P.gs, (unsigned)(++epoch), P.spin_limit, &s_ok)) { timed_out = true; break; }
         double rr[1] = { 0.0 };
         if (mine) {
             const int64_t sb = __ldg(P.slice_ptr + s);
             const V3 ax = spmv_row(P.val + 9 * sb + lane, P.col + sb + lane, len, P.x4, P.x4, 0.0, true);
+            const V3 b = ldg3(P.b4, row);
             r64 = V3{ b.a - ax.a, b.b - ax.b, b.c - ax.c };
             rr[0] = rr[0] + r64.a * r64.a; rr[0] = rr[0] + r64.b * r64.b; rr[0] = rr[0] + r64.c * r64.c;
         }
@@ -282,9 +314,9 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
         rnorm = sqrt(rr[0]);
         if (reason == GSLAM_STOP_PQ_ZERO) break;
     }
-#undef HALO_R
-#undef HALO_W
-#undef HALO_S
+#undef PUB_Z
+#undef PUB_U
+#undef PUB_V
     if (mine) st3(P.x4, row, x);
     if (timed_out && threadIdx.x == 0) {
         P.res->timeout = 1;

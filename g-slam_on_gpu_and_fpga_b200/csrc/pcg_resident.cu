@@ -15,10 +15,12 @@
  * z and p in registers. Only what other CTAs need crosses L2 each iteration: p
  * (phase A) and z (phase B). Column indices are staged as CTA-local indices: a
  * CTA's own rows first, then its halo (the other CTAs' rows its blocks touch, a
- * list fixed at setup). In phase A every owner writes its p to shared memory and
- * all threads of the CTA together stage the halo's p from L2 in one parallel pass,
- * so the SpMV reads values and p from shared memory only — one L2 round trip per
- * phase instead of one per pair of blocks. Phases and reductions are those of pcg.cu:
+ * list fixed at setup). Right after each phase-B grid barrier every thread loads
+ * the z and previous p of one halo row from L2 while the reduction partials are
+ * summed (the two round trips overlap); in phase A every owner writes its p to
+ * shared memory and every thread the p of its halo row, so the SpMV reads values
+ * and p from shared memory only. Thread 0 alone advances the scalars (alpha,
+ * beta, the stopping test) and hands them to the CTA through shared memory. Phases and reductions are those of pcg.cu:
  *   A: p = z + beta p; q = A p (neighbours' p recomputed from their z and old p,
  *      bit-identically); partial p.q                      -> grid reduction
  *   B: x += alpha p; r -= alpha q; z = D^-1 r; partial r.r, r.z -> grid reduction
@@ -41,6 +43,10 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     __shared__ double s_red[3][BS / 32];
     __shared__ double s_bc[4];
     __shared__ int s_ok;
+    /* scalars, advanced by thread 0 only: r.z, r.r, tol; alpha or beta; stop flag */
+    __shared__ double s_sc[3];
+    __shared__ double s_coef;
+    __shared__ int s_flag;
     __shared__ __align__(8) uint64_t s_bar;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int epoch = 0;
@@ -90,6 +96,13 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     const double *gval = P.val + 9 * slot0;  /* global copy of this CTA's share */
     const int *cb = scol + lslot + lane;
 
+    /* the halo row whose z and previous p this thread prefetches after each phase-B
+     * barrier (rows beyond the CTA's thread count are read in phase A instead) */
+    const int hh = h0 + (int)threadIdx.x;
+    const bool has_h = hh < h1;
+    const int hrow = has_h ? __ldg(P.halo_rows + hh) : 0;
+    V3 hz = { 0.0, 0.0, 0.0 }, hp = { 0.0, 0.0, 0.0 };
+
     V3 x = { 0.0, 0.0, 0.0 }, r = { 0.0, 0.0, 0.0 }, z = { 0.0, 0.0, 0.0 }, pn = { 0.0, 0.0, 0.0 };
     double acc2[2] = { 0.0, 0.0 };
     if (mine) {
@@ -99,14 +112,15 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
         acc2[0] = acc2[0] + r.a * z.a; acc2[0] = acc2[0] + r.b * z.b; acc2[0] = acc2[0] + r.c * z.c;
         acc2[1] = acc2[1] + r.a * r.a; acc2[1] = acc2[1] + r.b * r.b; acc2[1] = acc2[1] + r.c * r.c;
     }
-    if (!grid_allreduce<2, BS>(acc2, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
+    if (!grid_reduce_arrive<2, BS>(acc2, P.partials, epoch, P.gs, P.spin_limit, s_red, &s_ok)) {
         if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
         return;
     }
-    double rz = acc2[0];
+    if (has_h) hz = ldcg3(P.z4, hrow);
+    grid_reduce_collect<2, BS>(acc2, P.partials, epoch, s_bc);
     const double bnorm = sqrt(acc2[1]);
-    const double tol = P.tol_rel * bnorm;
-    double beta = 0.0, rr = acc2[1];
+    if (threadIdx.x == 0) { s_sc[0] = acc2[0]; s_sc[1] = acc2[1]; s_sc[2] = P.tol_rel * bnorm; }
+    double beta = 0.0;
     int k = 0, reason = GSLAM_STOP_MAXIT;
 
     while (true) {
@@ -123,7 +137,10 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
             st3(pnew, row, pn);
             st3(sp, row - row0, pn);
         }
-        for (int h = h0 + (int)threadIdx.x; h < h1; h += BS)
+        if (has_h)
+            st3(sp, n_loc + (int)threadIdx.x,
+                first ? hz : V3{ hz.a + beta * hp.a, hz.b + beta * hp.b, hz.c + beta * hp.c });
+        for (int h = hh + BS; h < h1; h += BS)
             st3(sp, n_loc + (h - h0), p_of(P.z4, pold, __ldg(P.halo_rows + h), beta, first));
         __syncthreads();
         if (mine) {
@@ -143,12 +160,18 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
             q = V3{ q0, q1, q2 };
             pq[0] = pq[0] + pn.a * q.a; pq[0] = pq[0] + pn.b * q.b; pq[0] = pq[0] + pn.c * q.c;
         }
-        if (!grid_allreduce<1, BS>(pq, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
+        if (!grid_reduce_arrive<1, BS>(pq, P.partials, epoch, P.gs, P.spin_limit, s_red, &s_ok)) {
             reason = GSLAM_STOP_TIMEOUT;
             break;
         }
-        if (pq[0] == 0.0) { reason = GSLAM_STOP_PQ_ZERO; break; }
-        const double alpha = rz / pq[0];
+        grid_reduce_sum<1>(P.partials, epoch, s_bc);
+        if (threadIdx.x == 0) {
+            s_flag = s_bc[0] == 0.0;
+            s_coef = s_sc[0] / s_bc[0];
+        }
+        __syncthreads();
+        if (s_flag) { reason = GSLAM_STOP_PQ_ZERO; break; }
+        const double alpha = s_coef;
         /* ---- phase B ---- */
         double rs[2] = { 0.0, 0.0 };
         if (mine) {
@@ -159,15 +182,24 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
             st3(P.z4, row, z);
             rs[1] = rs[1] + r.a * z.a; rs[1] = rs[1] + r.b * z.b; rs[1] = rs[1] + r.c * z.c;
         }
-        if (!grid_allreduce<2, BS>(rs, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
+        if (!grid_reduce_arrive<2, BS>(rs, P.partials, epoch, P.gs, P.spin_limit, s_red, &s_ok)) {
             reason = GSLAM_STOP_TIMEOUT;
             break;
         }
+        /* the halo's z_{k+1} and p_k, in flight while the partials are summed */
+        if (has_h) { hz = ldcg3(P.z4, hrow); hp = ldcg3(pnew, hrow); }
+        grid_reduce_sum<2>(P.partials, epoch, s_bc);
         k++;
-        rr = rs[0];
-        if (sqrt(rr) < tol) { reason = GSLAM_STOP_TOL; break; }
-        beta = rs[1] / rz;
-        rz = rs[1];
+        if (threadIdx.x == 0) {
+            const double rr = s_bc[0], rz_new = s_bc[1];
+            s_sc[1] = rr;
+            s_flag = sqrt(rr) < s_sc[2];
+            s_coef = rz_new / s_sc[0];
+            s_sc[0] = rz_new;
+        }
+        __syncthreads();
+        if (s_flag) { reason = GSLAM_STOP_TOL; break; }
+        beta = s_coef;
     }
     if (mine) st3(P.x4, row, x);
     if (reason == GSLAM_STOP_TIMEOUT && threadIdx.x == 0) {
@@ -179,7 +211,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
         P.res->reason = reason;
         P.res->refinements = 0;
         P.res->timeout = 0;
-        P.res->rnorm = sqrt(rr);
+        P.res->rnorm = sqrt(s_sc[1]);
         P.res->bnorm = bnorm;
     }
 }
