@@ -1,11 +1,11 @@
 /*
  * pcg_static.cu — block-Jacobi PCG on a caller's device CSR that allocates nothing.
  *
- * Who this is for: callers that cannot allocate device memory at solve time — code
- * recording work into a CUDA graph, processes whose device memory is owned by
- * another allocator or budgeted up front (a serving process with a fixed pool, an
- * embedded controller), or a real-time loop that must not call cudaMalloc. Every
- * other entry point of the library allocates its buffers when a graph is created.
+ * Who this is for: callers that cannot allocate device memory at solve time —
+ * processes whose device memory is owned by another allocator or budgeted up front
+ * (a serving process with a fixed pool, an embedded controller), or a real-time
+ * loop that must not call cudaMalloc because it can block or fail. Every other
+ * entry point of the library allocates its buffers when a graph is created.
  *
  * The solver's scratch (work vectors, block-Jacobi inverses, reduction partials,
  * barrier counter, status) lives in one file-scope __device__ array of

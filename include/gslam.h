@@ -201,8 +201,8 @@ void gslam_free_log(gslam_log *log);
 /* ---- solve without any device allocation ---- */
 /*
  * No counterpart in the reference. For callers that cannot allocate device memory when
- * they solve: work being recorded into a CUDA graph, processes whose device memory is
- * owned by another allocator or fixed up front, real-time loops. Solves the reference's
+ * they solve: processes whose device memory is owned by another allocator or fixed up
+ * front, real-time loops in which an allocation could block or fail. Solves the reference's
  * system (scalar CSR of Omega, dim = 3 * poses, columns ascending within a row; all
  * pointers are device memory the caller owns) with block-Jacobi PCG in FP64
  * (||r|| < tol ||b|| or max_iter iterations, x overwritten) on `stream`

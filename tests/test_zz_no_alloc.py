@@ -1,9 +1,9 @@
 """The allocation-free solver entry point (gslam_pcg_solve_static).
 
-For callers that cannot allocate device memory while they solve — work recorded
-into a CUDA graph, processes whose device memory belongs to another allocator or
-is fixed up front — the library offers one entry point whose scratch lives in a
-fixed array inside the library. This test calls it through the C ABI twice in a
+For callers that cannot allocate device memory while they solve — processes whose
+device memory belongs to another allocator or is fixed up front, real-time loops in
+which an allocation could block or fail — the library offers one entry point whose
+scratch lives in a fixed array inside the library. This test calls it through the C ABI twice in a
 row on device buffers the test owns, and compares both results with what the
 regular solver entry point (pcg_solve_sparse, the reference's own signature)
 returns for the same system, with the converged-solve tolerance used by
