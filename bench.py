@@ -396,6 +396,27 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_ncu_case(args):
+    """A short, untimed solve of the bench workload for ncu captures: the solver runs
+    twice on the first round's system, with 50 and then 250 iterations (tolerance 0),
+    so per-iteration DRAM traffic is the difference of the two launches / 200."""
+    import torch
+    G = importlib.import_module(PKG)
+    G.build.build()
+    cg = workload(seed=1)
+    prec = G.abi.PREC_MIXED if args.ncu_case == "mixed" else G.abi.PREC_FP64
+    g = G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=LAMBDA,
+                             tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=prec)
+    g.linearise()
+    g.assemble()
+    for iters in (50, 250):
+        g.set_opts(precision=prec, tol=0.0, max_iter=iters, inner_max_iter=iters)
+        st = g.solve()
+        print(f"{args.ncu_case}: {st.iterations} iterations, {st.solve_ms:.3f} ms", flush=True)
+    torch.cuda.synchronize()
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -403,8 +424,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", choices=["fp64", "mixed"], default=None,
+                    help="run only two short solves of the workload (for ncu captures)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.ncu_case:
+        run_ncu_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -22,12 +22,6 @@ __device__ __forceinline__ unsigned atom_add_release_u32(unsigned *p, unsigned v
     return old;
 }
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 __device__ __forceinline__ int ld_relaxed_s32(const int *p) {
     int v;
     asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -37,32 +31,42 @@ __device__ __forceinline__ int ld_relaxed_s32(const int *p) {
 /*
  * Grid barrier on a monotonic arrival counter: barrier number `epoch` (1, 2, ...)
  * is complete when the counter reaches epoch * gridDim.x. One release atomic per
- * CTA (it orders the CTA's prior writes, made visible to thread 0 by the CTA
- * barrier), then acquire polling: the cheapest of the variants measured on B200
- * (about 2.1 us per grid reduction with 148 CTAs, including the partials read). The counter is zeroed before every launch, so
- * 2^32 / gridDim.x barriers fit in one solve. Returns false when the solve must be
- * abandoned (this wait ran out of time, or another CTA's did).
+ * CTA (it orders the CTA's prior writes, made visible to thread 0 by a CTA
+ * barrier before it), then polling: each poll reads the counter and the abort flag
+ * with relaxed loads that are in flight together (one L2 round trip per poll), and
+ * a fence.acq_rel after the counter is seen complete gives the acquire side. The
+ * counter is zeroed before every launch, so 2^32 / gridDim.x barriers fit in one
+ * solve. grid_barrier_t0 is thread 0's part alone (the caller has already made the
+ * CTA's writes visible to thread 0 and publishes *s_ok after it); grid_barrier is
+ * the whole-CTA form. Both report false when the solve must be abandoned (this wait
+ * ran out of time, or another CTA's did).
  */
+__device__ __forceinline__ void grid_barrier_t0(GridSync *gs, unsigned epoch, long long spin_limit, int *s_ok) {
+    int ok = 1;
+    const unsigned target = epoch * gridDim.x;
+    const unsigned arrived = atom_add_release_u32(&gs->count, 1u) + 1u;
+    if (arrived < target) {
+        const long long t0 = clock64();
+        while (true) {
+            const unsigned c = ld_relaxed_u32(&gs->count);
+            const int ab = ld_relaxed_s32(&gs->abort);
+            if (c >= target) break;
+            if (ab) { ok = 0; break; }
+            if (clock64() - t0 > spin_limit) {
+                atomicExch(&gs->abort, 1);
+                ok = 0;
+                break;
+            }
+        }
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    }
+    *s_ok = ok;
+}
+
 __device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned epoch, long long spin_limit,
                                              int *s_ok) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned target = epoch * gridDim.x;
-        const unsigned arrived = atom_add_release_u32(&gs->count, 1u) + 1u;
-        if (arrived < target) {
-            const long long t0 = clock64();
-            while (ld_acquire_u32(&gs->count) < target) {
-                if (ld_relaxed_s32(&gs->abort)) { ok = 0; break; }
-                if (clock64() - t0 > spin_limit) {
-                    atomicExch(&gs->abort, 1);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        *s_ok = ok;
-    }
+    if (threadIdx.x == 0) grid_barrier_t0(gs, epoch, spin_limit, s_ok);
     __syncthreads();
     return *s_ok != 0;
 }
@@ -72,8 +76,9 @@ __device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned epoch, long 
  * a caller can issue loads of data the other CTAs published before the barrier
  * while the partials are summed, and can derive scalars from the totals in one
  * thread instead of all of them:
- *   grid_reduce_arrive:  block sum of each thread's v[], one partial per CTA,
- *                        grid barrier (false: the solve must be abandoned);
+ *   grid_reduce_arrive:  block sum of each thread's v[] (warp shuffles, then warp 0
+ *                        over the warps), one partial per CTA, grid barrier
+ *                        (false: the solve must be abandoned);
  *   grid_reduce_sum:     warp i < NV sums the CTAs' partials of value i into
  *                        s_bc[i] (a lane's loads all in flight together, a fixed
  *                        order: lane-strided, then a shuffle tree), then a
@@ -100,13 +105,26 @@ __device__ __forceinline__ bool grid_reduce_arrive(const double (&v)[NV], double
         if (lane == 0) s_red[i][warp] = a;
     }
     __syncthreads();
-    if (warp < NV) {
-        double a = lane < BS / 32 ? s_red[warp][lane] : 0.0;
+    if (warp == 0) {
+        /* warp 0 sums every value's per-warp partials (the trees interleave), and
+         * its lane 0 stores them and arrives: no second CTA barrier before the
+         * arrival, since the one above already ordered every thread's writes */
+        double a[NV];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a = a + __shfl_down_sync(0xffffffffu, a, o);
-        if (lane == 0) partials[warp * gridDim.x + blockIdx.x] = a;
+        for (int i = 0; i < NV; i++) a[i] = lane < BS / 32 ? s_red[i][lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int i = 0; i < NV; i++) a[i] = a[i] + __shfl_down_sync(0xffffffffu, a[i], o);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int i = 0; i < NV; i++) partials[i * gridDim.x + blockIdx.x] = a[i];
+            grid_barrier_t0(gs, (unsigned)epoch, spin_limit, s_ok);
+        }
     }
-    return grid_barrier(gs, (unsigned)epoch, spin_limit, s_ok);
+    __syncthreads();
+    return *s_ok != 0;
 }
 
 template <int NV>

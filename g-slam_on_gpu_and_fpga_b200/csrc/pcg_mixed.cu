@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     __shared__ int s_ok;
     __shared__ __align__(8) uint64_t s_bar;
     /* scalar recurrence, kept and advanced by thread 0 only (no registers in the
-     * other threads): gamma_{k-1}, alpha_{k-1}, rho_0 of the inner solve, tol */
-    __shared__ double s_sc[4];
+     * other threads): gamma_{k-1}, alpha_{k-1}, rho_0 of the inner solve, tol, ||xi|| */
+    __shared__ double s_sc[5];
     __shared__ float s_ab[2];  /* alpha, beta for the next iteration */
     __shared__ int s_flag;     /* 0 continue, 1 inner solve done, 2 breakdown */
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -158,9 +158,9 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     const int j_sm = min(len, max(0, ((int)nsm - 9 * lslot) / 288));
     /* the halo row this thread advances every iteration (more, in a loop, only when
      * the halo has more rows than the CTA has threads) */
-    const int hh = h0 + (int)threadIdx.x;
-    const bool has_h = hh < h1;
-    const int hrow = has_h ? __ldg(P.halo_rows + hh) : 0;
+    const bool has_h = (int)threadIdx.x < h1 - h0;
+    const int hrow = has_h ? __ldg(P.halo_rows + h0 + threadIdx.x) : 0;
+    const bool h_extra = h1 - h0 > BS;  /* CTA-uniform */
 
     /* published (z_k, u_k, v_{k-1}) in global memory, double-buffered by iteration
      * parity (selected with ?: so no local-memory array is needed) */
@@ -178,17 +178,19 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
         if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
         return;
     }
-    const double bnorm = sqrt(bb[0]);
-    if (threadIdx.x == 0) s_sc[3] = P.tol_rel * bnorm;
+    if (threadIdx.x == 0) {
+        s_sc[3] = P.tol_rel * sqrt(bb[0]);
+        s_sc[4] = sqrt(bb[0]);
+    }
 
     V3 x = { 0.0, 0.0, 0.0 };   /* FP64 solution (P.x4 holds it during an inner solve) */
     V3 r64 = mine ? ldg3(P.b4, row) : V3{ 0.0, 0.0, 0.0 }; /* FP64 residual, = xi for x = 0 */
-    double rnorm = bnorm;
+    double rnorm = sqrt(bb[0]);
     int total = 0, outer = 0, reason = GSLAM_STOP_MAXIT;
     bool timed_out = false;
 
     while (true) {
-        if (rnorm < P.tol_rel * bnorm) { reason = GSLAM_STOP_TOL; break; }
+        if (rnorm < P.tol_rel * s_sc[4]) { reason = GSLAM_STOP_TOL; break; }
         if (total >= P.max_iter || outer >= P.max_refine) { reason = GSLAM_STOP_MAXIT; break; }
         outer++;
         /* ---- inner FP32 solve of A d = r64; x += d in FP64 afterwards ---- */
@@ -218,11 +220,15 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
                 step_zv(hz, hu, hv, alpha, beta, zn, vn);
                 stf3(sz, n_loc + (int)threadIdx.x, zn);
             }
-            for (int h = hh + BS; h < h1; h += BS) {
-                const int c = __ldg(P.halo_rows + h);
-                F3 zn, vn;
-                step_zv(ldcgf3(PUB_Z(pr), c), ldcgf3(PUB_U(pr), c), ldcgf3(PUB_V(pr), c), alpha, beta, zn, vn);
-                stf3(sz, n_loc + (h - h0), zn);
+            if (h_extra) {
+                /* halo rows beyond the CTA's thread count (bounds re-read: rare path) */
+                const int e0 = __ldg(P.halo_ptr + blockIdx.x), e1 = __ldg(P.halo_ptr + blockIdx.x + 1);
+                for (int h = e0 + (int)threadIdx.x + BS; h < e1; h += BS) {
+                    const int c = __ldg(P.halo_rows + h);
+                    F3 zn, vn;
+                    step_zv(ldcgf3(PUB_Z(pr), c), ldcgf3(PUB_U(pr), c), ldcgf3(PUB_V(pr), c), alpha, beta, zn, vn);
+                    stf3(sz, n_loc + (h - e0), zn);
+                }
             }
             /* own row: s_{k-1}, r_k, p_{k-1}, d, then v_{k-1}, z_k */
             sv = axpy_f(beta, sv, w);
@@ -240,8 +246,11 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
                 int j = 0;
                 for (; j < j_sm; j++)
                     blk_acc_f(sval + 9 * lslot + 288 * j + lane, ldf3(sz, cb[32 * j]), q0, q1, q2);
-                for (; j < len; j++)
-                    blk_acc_f(P.val32 + 9 * (slot0 + lslot) + 288 * j + lane, ldf3(sz, cb[32 * j]), q0, q1, q2);
+                if (j < len) {
+                    /* blocks beyond the shared-memory share: values from L2 */
+                    const float *gv = P.val32 + 9 * __ldg(P.slice_ptr + s) + lane;
+                    for (; j < len; j++) blk_acc_f(gv + 288 * j, ldf3(sz, cb[32 * j]), q0, q1, q2);
+                }
                 w = F3{ q0, q1, q2 };
                 u = dinv_apply_f(sdinv + 288 * warp + lane, w); /* own row's D^-1 (stride 32) */
                 const double r0 = r.a, r1 = r.b, r2 = r.c, z0 = z.a, z1 = z.b, z2 = z.c;
@@ -266,8 +275,15 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
                 const double gamma = s_bc[0], delta = s_bc[1], rho = s_bc[2];
                 if (k == 1) s_sc[2] = rho;
                 double a, bt;
+                /* alpha_k = gamma / (delta - beta_k gamma / alpha_{k-1}) rewritten with
+                 * g = gamma_{k-1} alpha_{k-1}, so one division is on the critical path
+                 * (beta's runs beside it) */
                 if (k == 1) { bt = 0.0; a = gamma / delta; }
-                else { bt = gamma / s_sc[0]; a = gamma / (delta - bt * gamma / s_sc[1]); }
+                else {
+                    const double g = s_sc[0] * s_sc[1];
+                    bt = gamma / s_sc[0];
+                    a = (gamma * g) / (delta * g - gamma * gamma);
+                }
                 int flag = 0;
                 if (!(delta != 0.0) || !(a == a)) flag = 2;
                 else if (rho <= P.inner_tol * P.inner_tol * s_sc[2] || k >= P.inner_max_iter ||
@@ -317,7 +333,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
 #undef PUB_Z
 #undef PUB_U
 #undef PUB_V
-    if (mine) st3(P.x4, row, x);
+    /* P.x4 already holds x: stored at the start of every refinement step and after it */
     if (timed_out && threadIdx.x == 0) {
         P.res->timeout = 1;
         P.res->reason = GSLAM_STOP_TIMEOUT;
@@ -328,7 +344,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
         P.res->refinements = outer;
         P.res->timeout = 0;
         P.res->rnorm = rnorm;
-        P.res->bnorm = bnorm;
+        P.res->bnorm = s_sc[4];
     }
 }
 
