@@ -244,8 +244,18 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
                 float q0 = 0.f, q1 = 0.f, q2 = 0.f;
                 const int *cb = scol + lslot + lane;
                 int j = 0;
-                for (; j < j_sm; j++)
-                    blk_acc_f(sval + 9 * lslot + 288 * j + lane, ldf3(sz, cb[32 * j]), q0, q1, q2);
+                /* four blocks at a time: their column and z loads are in flight together
+                 * (a row's blocks are still added in ascending column order) */
+                const float *sv0 = sval + 9 * lslot + lane;
+                for (; j + 3 < j_sm; j += 4) {
+                    const int c0 = cb[32 * j], c1 = cb[32 * (j + 1)], c2 = cb[32 * (j + 2)], c3 = cb[32 * (j + 3)];
+                    const F3 z0 = ldf3(sz, c0), z1 = ldf3(sz, c1), z2 = ldf3(sz, c2), z3 = ldf3(sz, c3);
+                    blk_acc_f(sv0 + 288 * j, z0, q0, q1, q2);
+                    blk_acc_f(sv0 + 288 * (j + 1), z1, q0, q1, q2);
+                    blk_acc_f(sv0 + 288 * (j + 2), z2, q0, q1, q2);
+                    blk_acc_f(sv0 + 288 * (j + 3), z3, q0, q1, q2);
+                }
+                for (; j < j_sm; j++) blk_acc_f(sv0 + 288 * j, ldf3(sz, cb[32 * j]), q0, q1, q2);
                 if (j < len) {
                     /* blocks beyond the shared-memory share: values from L2 */
                     const float *gv = P.val32 + 9 * __ldg(P.slice_ptr + s) + lane;

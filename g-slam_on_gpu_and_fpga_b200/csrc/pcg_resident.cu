@@ -92,7 +92,9 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     const int row = 32 * s + lane;
     const bool mine = own_slice && row < P.n_rows;
     const int len = mine ? __ldg(P.row_len + row) : 0;
-    const int64_t lslot = own_slice ? (__ldg(P.slice_ptr + s) - slot0) : 0; /* local slot of (j=0) */
+    const int lslot = own_slice ? (int)(__ldg(P.slice_ptr + s) - slot0) : 0; /* local slot of (j=0) */
+    /* how many of the row's blocks have their values in shared memory */
+    const int j_sm = min(len, max(0, ((int)nsm - 9 * lslot) / 288));
     const double *gval = P.val + 9 * slot0;  /* global copy of this CTA's share */
     const int *cb = scol + lslot + lane;
 
@@ -145,17 +147,28 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
         __syncthreads();
         if (mine) {
             double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+            /* blocks with values in shared memory, four at a time (their column and p
+             * loads in flight together), then the share's tail from L2, two at a time;
+             * a row's blocks are added in ascending column order either way */
+            const double *sv0 = sval + 9 * lslot + lane;
             int j = 0;
-            for (; j + 1 < len; j += 2) {
-                const V3 p0 = ld3(sp, cb[32 * j]), p1 = ld3(sp, cb[32 * (j + 1)]);
-                const int64_t o0 = 9 * lslot + 288 * j, o1 = o0 + 288;
-                blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
-                blk_acc_any(o1 + 288 <= nsm ? sval + o1 + lane : gval + o1 + lane, p1, q0, q1, q2);
+            for (; j + 3 < j_sm; j += 4) {
+                const int c0 = cb[32 * j], c1 = cb[32 * (j + 1)], c2 = cb[32 * (j + 2)], c3 = cb[32 * (j + 3)];
+                const V3 p0 = ld3(sp, c0), p1 = ld3(sp, c1), p2 = ld3(sp, c2), p3 = ld3(sp, c3);
+                blk_acc_any(sv0 + 288 * j, p0, q0, q1, q2);
+                blk_acc_any(sv0 + 288 * (j + 1), p1, q0, q1, q2);
+                blk_acc_any(sv0 + 288 * (j + 2), p2, q0, q1, q2);
+                blk_acc_any(sv0 + 288 * (j + 3), p3, q0, q1, q2);
             }
+            for (; j < j_sm; j++) blk_acc_any(sv0 + 288 * j, ld3(sp, cb[32 * j]), q0, q1, q2);
             if (j < len) {
-                const V3 p0 = ld3(sp, cb[32 * j]);
-                const int64_t o0 = 9 * lslot + 288 * j;
-                blk_acc_any(o0 + 288 <= nsm ? sval + o0 + lane : gval + o0 + lane, p0, q0, q1, q2);
+                const double *gv = gval + 9 * lslot + lane;
+                for (; j + 1 < len; j += 2) {
+                    const V3 p0 = ld3(sp, cb[32 * j]), p1 = ld3(sp, cb[32 * (j + 1)]);
+                    blk_acc(gv + 288 * j, p0, q0, q1, q2);
+                    blk_acc(gv + 288 * (j + 1), p1, q0, q1, q2);
+                }
+                if (j < len) blk_acc(gv + 288 * j, ld3(sp, cb[32 * j]), q0, q1, q2);
             }
             q = V3{ q0, q1, q2 };
             pq[0] = pq[0] + pn.a * q.a; pq[0] = pq[0] + pn.b * q.b; pq[0] = pq[0] + pn.c * q.c;
