@@ -37,7 +37,7 @@ EXPORTS = [
     "gslam_version", "gslam_last_error", "gslam_obs_edge_order", "gslam_csr_pattern",
     "pcg_solve_sparse", "device_graph_init", "device_graph_update", "device_graph_get_row_ptr",
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
-    "gslam_dropin_status", "gslam_pcg_solve_static",
+    "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_set_se2_weights", "gslam_adjoint",
 ]
 
 
@@ -155,6 +155,8 @@ def lib() -> C.CDLL:
             "gslam_dropin_status": [],
             "gslam_pcg_solve_static": [C.c_int, VP, VP, VP, VP, VP, C.c_double, C.c_int, VP,
                                        C.POINTER(SolveStats)],
+            "gslam_set_se2_weights": [VP, C.c_double, DP],
+            "gslam_adjoint": [VP, DP, DP, DP, DP, C.POINTER(SolveStats)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

@@ -77,6 +77,7 @@ struct gslam_graph {
     double *d_dx = nullptr, *d_block_sums = nullptr, *d_diff = nullptr;
     int n_upd_blocks = 1;
     double *d_csr_tmp = nullptr, *d_xi_tmp = nullptr;
+    double *d_adj = nullptr;   /* adjoint: rhs, mu (3 N each), per-edge gradient (3 E) */
     PcgResult *h_res = nullptr;
     double *h_diff = nullptr;
     PcgResult last_res = {};

@@ -234,6 +234,27 @@ class PoseGraph:
         abi.check(abi.lib().gslam_get_dx(self._h, abi.ptr(out)))
         return out
 
+    # ---- differentiation (SE(2) graphs) ----
+    def set_weights(self, lam: float, log_w=None) -> None:
+        """New lambda and (optionally) per-edge log information weights [E, 3]."""
+        lw = None if log_w is None else np.ascontiguousarray(log_w, np.float64).reshape(-1)
+        abi.check(abi.lib().gslam_set_se2_weights(self._h, float(lam),
+                                                  abi.ptr(lw) if lw is not None else None))
+
+    def adjoint(self, dL_dposes):
+        """Implicit-function adjoint at the current (converged) poses: returns
+        (dL/dlambda, dL/dlog_w [E, 3], mu [N, 3], RoundStats of the adjoint solve)."""
+        g = np.ascontiguousarray(dL_dposes, np.float64).reshape(self.n_poses, 3)
+        n_e = self.sizes()["n_edges"]
+        dlw = np.zeros((n_e, 3))
+        mu = np.zeros((self.n_poses, 3))
+        dlam = C.c_double()
+        st = abi.SolveStats()
+        abi.check(abi.lib().gslam_adjoint(self._h, abi.ptr(g), C.byref(dlam), abi.ptr(dlw), abi.ptr(mu),
+                                          C.byref(st)))
+        return dlam.value, dlw, mu, RoundStats(st.iterations, st.refinements, st.reason, st.rel_residual,
+                                               st.diff, st.solve_ms)
+
     def diag_inv(self) -> np.ndarray:
         out = np.zeros((self.n_poses, 9))
         abi.check(abi.lib().gslam_get_diag_inv(self._h, abi.ptr(out)))

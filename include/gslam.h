@@ -221,6 +221,28 @@ int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *d_col_idx,
                            const double *d_values, const double *d_b, double *d_x, double tol,
                            int max_iter, void *stream, gslam_solve_stats *stats);
 
+/*
+ * Differentiation of a converged SE(2) graph (no counterpart in the reference, whose
+ * programs only run Gauss-Newton forward).
+ *
+ * gslam_set_se2_weights: replaces lambda and, when log_w is non-null, the per-edge
+ * log information weights (3 per edge, edge order of gslam_create_se2) of an SE(2)
+ * graph; the block structure is kept.
+ *
+ * gslam_adjoint: implicit-function adjoint at the graph's current poses, which should
+ * be converged (g(x) = sum_e J_e^T Lambda_e e_e = 0). Solves H mu = dL/dposes with the
+ * FP64 persistent PCG (the graph's tol / max_iter; H = the exact Hessian of
+ * (1/2) sum_e e^T Lambda_e e, symmetric, pose-0 anchor included), then
+ *   dL_dlogw[3e + k] = -lambda exp(w_{e,k}) e_{e,k} (J_e mu)_k   (host, 3 per edge),
+ *   *dL_dlambda      = sum of dL_dlogw / lambda                   (host),
+ * mu_out (host, 3 N, may be NULL) receives mu. dL_dposes is host memory, 3 N doubles,
+ * pose-major. The graph's assembled Omega / xi are overwritten; the next round
+ * re-linearises. Reference-factor graphs return GSLAM_ERR_BAD_INPUT.
+ */
+int gslam_set_se2_weights(gslam_graph *g, double lambda, const double *log_w);
+int gslam_adjoint(gslam_graph *g, const double *dL_dposes, double *dL_dlambda, double *dL_dlogw,
+                  double *mu_out, gslam_solve_stats *stats);
+
 /* Library version string and the error text of the last failing call on this thread. */
 const char *gslam_version(void);
 const char *gslam_last_error(void);

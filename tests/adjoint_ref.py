@@ -1,0 +1,108 @@
+"""Dense FP64 reference for the SE(2) Gauss-Newton solve and its implicit-function
+adjoint (test infrastructure; numpy only).
+
+Same factor and conventions as the library (csrc/edge_math.cuh em_se2_edge, csrc/adjoint.cu):
+  e = [R(th_i)^T (t_j - t_i) - z_t ; wrap(th_j - th_i - z_th)],  Lambda = lambda diag(exp(w)),
+  Omega = sum J^T Lambda J + anchor on pose 0's diagonal, xi = -sum J^T Lambda e,
+  poses += Omega^-1 xi with the angle wrapped.
+Adjoint at converged poses: H mu = dL/dx with H the exact Hessian of
+(1/2) sum e^T Lambda e (+ anchor), dL/dw_{e,k} = -Lambda_k e_k (J mu)_k,
+dL/dlambda = sum dL/dw / lambda.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def wrap(a):
+    return (a + np.pi) % (2.0 * np.pi) - np.pi
+
+
+def residuals(poses, ei, ej, meas):
+    """e [E, 3], J_i [E, 3, 3], J_j [E, 3, 3], plus (c, s, dx, dy) for the Hessian terms."""
+    pi, pj = poses[ei], poses[ej]
+    c, s = np.cos(pi[:, 2]), np.sin(pi[:, 2])
+    dx, dy = pj[:, 0] - pi[:, 0], pj[:, 1] - pi[:, 1]
+    e = np.stack([c * dx + s * dy - meas[:, 0], c * dy - s * dx - meas[:, 1],
+                  wrap(pj[:, 2] - pi[:, 2] - meas[:, 2])], axis=1)
+    n = len(ei)
+    Ji = np.zeros((n, 3, 3))
+    Jj = np.zeros((n, 3, 3))
+    Ji[:, 0] = np.stack([-c, -s, c * dy - s * dx], axis=1)
+    Ji[:, 1] = np.stack([s, -c, -c * dx - s * dy], axis=1)
+    Ji[:, 2, 2] = -1.0
+    Jj[:, 0, 0], Jj[:, 0, 1] = c, s
+    Jj[:, 1, 0], Jj[:, 1, 1] = -s, c
+    Jj[:, 2, 2] = 1.0
+    return e, Ji, Jj, (c, s, dx, dy)
+
+
+def _scatter(H, ei, ej, UL, UR, BL, BR):
+    for k in range(len(ei)):
+        i, j = 3 * ei[k], 3 * ej[k]
+        H[i:i + 3, i:i + 3] += UL[k]
+        H[i:i + 3, j:j + 3] += UR[k]
+        H[j:j + 3, i:i + 3] += BL[k]
+        H[j:j + 3, j:j + 3] += BR[k]
+
+
+def system(poses, ei, ej, meas, log_w, lam, anchor, exact=False):
+    """Dense Omega (or the exact Hessian) and xi = -g at `poses`."""
+    n = poses.shape[0]
+    e, Ji, Jj, (c, s, dx, dy) = residuals(poses, ei, ej, meas)
+    L = lam * np.exp(log_w)
+    LJi, LJj = L[:, :, None] * Ji, L[:, :, None] * Jj
+    UL = np.einsum("eki,ekj->eij", Ji, LJi)
+    UR = np.einsum("eki,ekj->eij", Ji, LJj)
+    BL = np.einsum("eki,ekj->eij", Jj, LJi)
+    BR = np.einsum("eki,ekj->eij", Jj, LJj)
+    if exact:
+        a0, a1 = L[:, 0] * e[:, 0], L[:, 1] * e[:, 1]
+        htt = a0 * (-c * dx - s * dy) + a1 * (s * dx - c * dy)
+        htx = a0 * s + a1 * c
+        hty = a1 * s - a0 * c
+        UL = UL.copy(); UR = UR.copy(); BL = BL.copy()
+        UL[:, 2, 2] += htt
+        UL[:, 2, 0] += htx; UL[:, 0, 2] += htx
+        UL[:, 2, 1] += hty; UL[:, 1, 2] += hty
+        UR[:, 2, 0] -= htx; UR[:, 2, 1] -= hty
+        BL[:, 0, 2] -= htx; BL[:, 1, 2] -= hty
+    H = np.zeros((3 * n, 3 * n))
+    _scatter(H, ei, ej, UL, UR, BL, BR)
+    H[0:3, 0:3] += anchor * np.eye(3)
+    Le = L * e
+    xi = np.zeros(3 * n)
+    np.add.at(xi.reshape(n, 3), ei, -np.einsum("eki,ek->ei", Ji, Le))
+    np.add.at(xi.reshape(n, 3), ej, -np.einsum("eki,ek->ei", Jj, Le))
+    return H, xi
+
+
+def gn_solve(poses0, ei, ej, meas, log_w, lam, anchor=1e6, rounds=50, tol=1e-13):
+    """Dense Gauss-Newton to convergence (update RMS below tol)."""
+    p = np.array(poses0, np.float64, copy=True)
+    for _ in range(rounds):
+        H, xi = system(p, ei, ej, meas, log_w, lam, anchor)
+        dx = np.linalg.solve(H, xi).reshape(-1, 3)
+        p = p + dx
+        p[:, 2] = wrap(p[:, 2])
+        if np.sqrt(np.mean(dx ** 2)) < tol:
+            break
+    return p
+
+
+def adjoint(poses, ei, ej, meas, log_w, lam, dL_dx, anchor=1e6):
+    """(dL/dlambda, dL/dlog_w [E, 3], mu [N, 3]) by a dense exact-Hessian solve."""
+    H, _ = system(poses, ei, ej, meas, log_w, lam, anchor, exact=True)
+    mu = np.linalg.solve(H, np.asarray(dL_dx, np.float64).reshape(-1)).reshape(-1, 3)
+    e, Ji, Jj, _ = residuals(poses, ei, ej, meas)
+    jm = np.einsum("ekc,ec->ek", Ji, mu[ei]) + np.einsum("ekc,ec->ek", Jj, mu[ej])
+    dlw = -(lam * np.exp(log_w)) * e * jm
+    return dlw.sum() / lam, dlw, mu
+
+
+def position_loss(poses, target):
+    """Sum of squared position differences, and its gradient w.r.t. the poses."""
+    d = poses[:, :2] - target[:, :2]
+    g = np.zeros_like(poses)
+    g[:, :2] = 2.0 * d
+    return float((d ** 2).sum()), g

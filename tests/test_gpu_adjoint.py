@@ -1,0 +1,116 @@
+"""GPU tests of the implicit-function adjoint (gslam_adjoint) and its
+torch.autograd.Function (autodiff.GNSolve) on an 800-pose city-grid graph.
+
+Checked against (1) the dense FP64 reference of tests/adjoint_ref.py evaluated at the
+GPU's converged poses, and (2) central finite differences (h = 1e-6 on the log
+weights) of the GPU Gauss-Newton solve on 32 seeded random (edge, component) pairs.
+Loss: sum of squared position differences to the noise-free walk.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+import adjoint_ref as R
+
+pytestmark = pytest.mark.gpu
+
+LAM = 0.1
+# Pose 0's anchor: the forward solve's gauge fix. The adjoint treats pose 0 as held by
+# it; with the default 1e6 (1000x the heading information here) Gauss-Newton lets pose 0
+# drift by ~1e-3 of each update, which changes with the weights and shows up in finite
+# differences at the 1e-3 level, so these tests pin pose 0 harder.
+ANCHOR = 1e12
+
+
+@pytest.fixture(scope="module")
+def setup(pkg):
+    synth = importlib.import_module("g-slam_on_gpu_and_fpga_b200.synth")
+    cg = synth.city_grid(800, seed=2)
+    g = pkg.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=LAM, anchor=ANCHOR,
+                               tol=1e-13, max_iter=40000, angle_wrap=1)
+    yield cg, g
+    g.close()
+
+
+def converge(g, cg, log_w, lam=LAM, rounds=40, start=None, min_rounds=1):
+    """Gauss-Newton to convergence from the initial guess, or from `start` (the
+    finite differences restart from the converged poses: the fixpoint is the same,
+    and the solve noise then scales with the perturbation, not with the problem).
+    Gauss-Newton converges linearly here (it omits the second-order terms the exact
+    Hessian has), so a restart takes at least `min_rounds` rounds even when the
+    first update is already below the stopping threshold."""
+    g.set_weights(lam, log_w)
+    g.poses = cg.init if start is None else start
+    for r in range(rounds):
+        st = g.round()
+        if st.diff < 1e-12 and r + 1 >= min_rounds:
+            break
+    return g.poses
+
+
+def test_adjoint_matches_dense_reference(setup):
+    cg, g = setup
+    p = converge(g, cg, cg.log_w)
+    _, dL = R.position_loss(p, cg.gt)
+    dlam, dlw, mu, st = g.adjoint(dL)
+    assert st.rel_residual < 1e-10
+    rlam, rdlw, rmu = R.adjoint(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAM, dL, anchor=ANCHOR)
+    assert np.linalg.norm(mu - rmu) <= 1e-8 * np.linalg.norm(rmu)
+    assert np.linalg.norm(dlw - rdlw) <= 1e-8 * np.linalg.norm(rdlw)
+    assert abs(dlam - rlam) <= 1e-8 * np.abs(rdlw).sum() / LAM
+
+
+@pytest.mark.parametrize("h,rel", [(1e-3, 1e-5), (1e-6, 2e-3)])
+def test_adjoint_matches_finite_differences(setup, h, rel):
+    """Central differences of the loss on 32 seeded (edge, component) pairs.
+
+    The converged poses are fixed only to the FP64 accuracy of the fixpoint
+    (|xi| ~ 3e-11 here, poses to ~1e-11..1e-9 through the conditioning), which puts
+    noise of ~1e-9 / (2 h) into each difference: with h = 1e-6 that is ~5e-4 absolute
+    (the dense CPU solver shows the same), so h = 1e-6 is checked at that noise level
+    and h = 1e-3 (truncation O(h^2) ~ 1e-6, noise ~ 5e-7) at 1e-5 relative."""
+    cg, g = setup
+    p = converge(g, cg, cg.log_w)
+    _, dL = R.position_loss(p, cg.gt)
+    _, dlw, _, _ = g.adjoint(dL)
+    rng = np.random.default_rng(7)
+    fd, adj = [], []
+    for _ in range(32):
+        e, k = int(rng.integers(len(cg.edge_i))), int(rng.integers(3))
+        lw1, lw2 = cg.log_w.copy(), cg.log_w.copy()
+        lw1[e, k] += h
+        lw2[e, k] -= h
+        lp = R.position_loss(converge(g, cg, lw1, start=p, min_rounds=12), cg.gt)[0]
+        lm = R.position_loss(converge(g, cg, lw2, start=p, min_rounds=12), cg.gt)[0]
+        fd.append((lp - lm) / (2 * h))
+        adj.append(dlw[e, k])
+    fd, adj = np.array(fd), np.array(adj)
+    assert np.linalg.norm(fd - adj) <= rel * np.linalg.norm(adj), (fd, adj)
+
+
+def test_autograd_function(setup, pkg):
+    import torch
+    autodiff = importlib.import_module("g-slam_on_gpu_and_fpga_b200.autodiff")
+    cg, g = setup
+    lam = torch.tensor(LAM, dtype=torch.float64, requires_grad=True)
+    log_w = torch.tensor(cg.log_w, dtype=torch.float64, requires_grad=True)
+    poses = autodiff.gn_solve(lam, log_w, g, cg.init, 40, 1e-12)
+    target = torch.from_numpy(cg.gt)
+    loss = ((poses[:, :2] - target[:, :2]) ** 2).sum()
+    loss.backward()
+    p = poses.detach().numpy()
+    _, dL = R.position_loss(p, cg.gt)
+    rlam, rdlw, _ = R.adjoint(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAM, dL, anchor=ANCHOR)
+    assert np.linalg.norm(log_w.grad.numpy() - rdlw) <= 1e-8 * np.linalg.norm(rdlw)
+    assert abs(lam.grad.item() - rlam) <= 1e-8 * np.abs(rdlw).sum() / LAM
+
+
+def test_adjoint_rejects_reference_factor_graphs(pkg):
+    synth = importlib.import_module("g-slam_on_gpu_and_fpga_b200.synth")
+    cg = synth.city_grid(64, seed=3)
+    log = synth.to_reference_log(cg)
+    g = pkg.PoseGraph.from_log(log, 1.0)
+    with pytest.raises(pkg.abi.GslamError):
+        g.adjoint(np.zeros((g.n_poses, 3)))
+    g.close()
