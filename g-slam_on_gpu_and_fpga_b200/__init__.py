@@ -10,4 +10,4 @@ The directory name is not a Python identifier; import it with
 importlib.import_module("g-slam_on_gpu_and_fpga_b200").
 """
 from . import abi, build, graph, synth  # noqa: F401
-from .graph import PoseGraph, ReferenceLog, RoundStats, read_log  # noqa: F401
+from .graph import PoseGraph, PoseGraphBatch, ReferenceLog, RoundStats, read_log  # noqa: F401

@@ -38,6 +38,7 @@ EXPORTS = [
     "pcg_solve_sparse", "device_graph_init", "device_graph_update", "device_graph_get_row_ptr",
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
     "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_set_se2_weights", "gslam_adjoint",
+    "gslam_create_se2_batch", "gslam_batch_round", "gslam_batch_layout",
 ]
 
 
@@ -157,6 +158,9 @@ def lib() -> C.CDLL:
                                        C.POINTER(SolveStats)],
             "gslam_set_se2_weights": [VP, C.c_double, DP],
             "gslam_adjoint": [VP, DP, DP, DP, DP, C.POINTER(SolveStats)],
+            "gslam_create_se2_batch": [C.POINTER(SE2GraphDesc), C.c_uint32, C.POINTER(Opts), C.POINTER(VP)],
+            "gslam_batch_round": [VP, C.POINTER(SolveStats)],
+            "gslam_batch_layout": [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

@@ -132,7 +132,10 @@ static inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / 
 
 int gslam_set_se2_weights(gslam_graph *g, double lambda, const double *log_w) {
     if (!g) { gslam_set_last_error("null handle"); return GSLAM_ERR_BAD_INPUT; }
-    if (g->factors != GSLAM_FACTORS_SE2) { gslam_set_last_error("weights belong to SE(2) graphs"); return GSLAM_ERR_BAD_INPUT; }
+    if (g->factors != GSLAM_FACTORS_SE2 || g->batch) {
+        gslam_set_last_error("weights can be replaced on single SE(2) graphs");
+        return GSLAM_ERR_BAD_INPUT;
+    }
     if (!(lambda > 0.0)) { gslam_set_last_error("lambda must be positive"); return GSLAM_ERR_BAD_INPUT; }
     g->lambda = lambda;
     if (log_w && g->n_edges) {
@@ -149,7 +152,10 @@ int gslam_set_se2_weights(gslam_graph *g, double lambda, const double *log_w) {
 int gslam_adjoint(gslam_graph *g, const double *dL_dposes, double *dL_dlambda, double *dL_dlogw,
                   double *mu_out, gslam_solve_stats *stats) {
     if (!g || !dL_dposes) { gslam_set_last_error("null argument"); return GSLAM_ERR_BAD_INPUT; }
-    if (g->factors != GSLAM_FACTORS_SE2) { gslam_set_last_error("the adjoint is defined for SE(2) graphs"); return GSLAM_ERR_BAD_INPUT; }
+    if (g->factors != GSLAM_FACTORS_SE2 || g->batch) {
+        gslam_set_last_error("the adjoint is defined for single SE(2) graphs");
+        return GSLAM_ERR_BAD_INPUT;
+    }
     const int n = g->n_poses;
     const int64_t ne = g->n_edges;
     cudaError_t ce = cudaSetDevice(g->device);

@@ -53,6 +53,27 @@ struct DevLayout {
     int max_grid_alloc() const { return partial_capacity; }
 };
 
+/* A batch of independent SE(2) graphs as one block-diagonal graph (batch.cu). */
+struct BatchState {
+    int n_graphs = 0;
+    std::vector<int> pose_off;   /* [n_graphs + 1] first (padded) pose of each graph */
+    std::vector<int> n_real;     /* [n_graphs] poses of each graph without padding */
+    int *d_pose_off = nullptr, *d_n_real = nullptr;
+    int n_anchor = 0;
+    int64_t *d_anchor_slots = nullptr;
+    double *d_anchor_vals = nullptr;
+    /* solver partition */
+    int grid = 0, block = 0, max_slices = 0;
+    size_t smem_bytes = 0;
+    int total_parts = 0;
+    int *d_cta_slice = nullptr, *d_slice_graph = nullptr, *d_cta_g0 = nullptr, *d_cta_g1 = nullptr;
+    int *d_graph_cta0 = nullptr, *d_graph_ncta = nullptr, *d_part_off = nullptr;
+    double *d_partials = nullptr, *d_gdiff = nullptr;
+    PcgResult *d_res = nullptr, *h_res = nullptr;
+    double *h_gdiff = nullptr;
+    int *d_active = nullptr;
+};
+
 struct gslam_graph {
     int device = 0;
     cudaStream_t st = nullptr;
@@ -78,6 +99,7 @@ struct gslam_graph {
     int n_upd_blocks = 1;
     double *d_csr_tmp = nullptr, *d_xi_tmp = nullptr;
     double *d_adj = nullptr;   /* adjoint: rhs, mu (3 N each), per-edge gradient (3 E) */
+    BatchState *batch = nullptr; /* non-null for a batch of graphs */
     PcgResult *h_res = nullptr;
     double *h_diff = nullptr;
     PcgResult last_res = {};

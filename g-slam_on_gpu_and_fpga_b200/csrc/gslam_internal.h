@@ -56,11 +56,17 @@ struct gslam_structure {
 /* Layout of a sorted unique block-key pattern (keys I * N + J, (0,0) included). */
 int gslam_layout_from_blocks(int n_rows, const std::vector<uint64_t> &keys, bool bare_anchor,
                              int sell_window, gslam_structure *s,
-                             std::vector<int64_t> *key_slot_out);
+                             std::vector<int64_t> *key_slot_out,
+                             const std::vector<int> *segments = nullptr);
 
 /* Builds the structure from the edge list (t1[e], t2[e]) in array order. */
 int gslam_build_structure(int n_rows, int64_t n_edges, const unsigned *t1, const unsigned *t2,
                           int sell_window, gslam_structure *s);
+/* Same, with extra diagonal blocks (rows that have no edge, e.g. a batch's padding
+ * poses) and segment starts at which the row-sorting windows restart. */
+int gslam_build_structure_ex(int n_rows, int64_t n_edges, const unsigned *t1, const unsigned *t2,
+                             int sell_window, const std::vector<int> *diag_rows,
+                             const std::vector<int> *segments, gslam_structure *s);
 
 /* Reference edge order for observation edges (GSLAM.c:222-318): pairs of z-list indices. */
 void gslam_obs_pairs(int64_t n_z, const unsigned *z_lm, std::vector<unsigned> *pj,

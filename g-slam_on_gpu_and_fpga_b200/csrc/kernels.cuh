@@ -85,6 +85,28 @@ struct PcgParams {
     int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
 };
 
+/* Batched solver (batch.cu): per-graph scalars over a block-diagonal system. */
+struct BatchParams {
+    int n_graphs;
+    const int *cta_slice;    /* [grid + 1] first slice of each CTA */
+    const int *slice_graph;  /* [n_slices] graph of each slice */
+    const int *cta_g0, *cta_g1; /* [grid] first / last graph of each CTA's slices */
+    const int *graph_cta0;   /* [n_graphs] first CTA owning rows of the graph */
+    const int *graph_ncta;   /* [n_graphs] CTAs owning rows of the graph */
+    const int *part_off;     /* [n_graphs] offset of the graph's CTA partials */
+    int total_parts;         /* sum of graph_ncta */
+    double *partials;        /* [2 buffers][2 values][total_parts] */
+    PcgResult *res;          /* [n_graphs] */
+    int *active;             /* graphs still iterating (set to n_graphs before launch) */
+};
+cudaError_t launch_pcg_batch(cudaStream_t st, const PcgParams &p, const BatchParams &b, int grid, int block,
+                             size_t smem_bytes);
+int pcg_batch_max_grid(int block, size_t smem_bytes, int device);
+int pcg_batch_lg_max();
+void launch_add_diag(cudaStream_t st, int n, const int64_t *slots, const double *anchor, double *val);
+void launch_batch_diff(cudaStream_t st, int n_graphs, const int *pose_off, const int *n_real, const double *dx,
+                       double *out);
+
 /* Cooperative launch of the persistent solver; returns the CUDA error. */
 cudaError_t launch_pcg(cudaStream_t st, const PcgParams &p, int precision, int grid, int block);
 /* Largest co-resident grid for the solver at this block size (0 if unsupported). */

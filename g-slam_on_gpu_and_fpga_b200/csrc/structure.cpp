@@ -64,7 +64,7 @@ void gslam_obs_pairs(int64_t n_z, const unsigned *z_lm, std::vector<unsigned> *p
  */
 int gslam_layout_from_blocks(int n_rows, const std::vector<uint64_t> &keys, bool bare_anchor,
                              int sell_window, gslam_structure *s,
-                             std::vector<int64_t> *key_slot_out) {
+                             std::vector<int64_t> *key_slot_out, const std::vector<int> *segments) {
     const uint64_t nb = (uint64_t)n_rows;
     s->n_rows = n_rows;
     s->bare_anchor = bare_anchor;
@@ -77,11 +77,17 @@ int gslam_layout_from_blocks(int n_rows, const std::vector<uint64_t> &keys, bool
     s->perm.resize(n_rows);
     std::iota(s->perm.begin(), s->perm.end(), 0);
     if (sell_window > 1) {
-        for (int w0 = 0; w0 < n_rows; w0 += sell_window) {
-            int w1 = std::min(n_rows, w0 + sell_window);
-            std::stable_sort(s->perm.begin() + w0, s->perm.begin() + w1, [&](int a, int b) {
-                return (rstart[a + 1] - rstart[a]) > (rstart[b + 1] - rstart[b]);
-            });
+        /* windows restart at every segment start (a batch keeps each graph's rows
+         * in its own, slice-aligned range) */
+        std::vector<int> seg = segments ? *segments : std::vector<int>{ 0 };
+        seg.push_back(n_rows);
+        for (size_t q = 0; q + 1 < seg.size(); q++) {
+            for (int w0 = seg[q]; w0 < seg[q + 1]; w0 += sell_window) {
+                int w1 = std::min(seg[q + 1], w0 + sell_window);
+                std::stable_sort(s->perm.begin() + w0, s->perm.begin() + w1, [&](int a, int b) {
+                    return (rstart[a + 1] - rstart[a]) > (rstart[b + 1] - rstart[b]);
+                });
+            }
         }
     }
     s->iperm.assign(n_rows, 0);
@@ -162,6 +168,12 @@ int gslam_layout_from_blocks(int n_rows, const std::vector<uint64_t> &keys, bool
 
 int gslam_build_structure(int n_rows, int64_t n_edges, const unsigned *t1, const unsigned *t2,
                           int sell_window, gslam_structure *s) {
+    return gslam_build_structure_ex(n_rows, n_edges, t1, t2, sell_window, nullptr, nullptr, s);
+}
+
+int gslam_build_structure_ex(int n_rows, int64_t n_edges, const unsigned *t1, const unsigned *t2,
+                             int sell_window, const std::vector<int> *diag_rows,
+                             const std::vector<int> *segments, gslam_structure *s) {
     if (n_rows <= 0) return GSLAM_ERR_BAD_INPUT;
     for (int64_t e = 0; e < n_edges; e++)
         if (t1[e] >= (unsigned)n_rows || t2[e] >= (unsigned)n_rows) return GSLAM_ERR_BAD_INPUT;
@@ -182,10 +194,15 @@ int gslam_build_structure(int n_rows, int64_t n_edges, const unsigned *t1, const
     for (int64_t e = 0; e < n_edges && bare; e++)
         if (t1[e] == 0 || t2[e] == 0) bare = false;
     keys.push_back(0); /* block (0,0) always exists internally: it carries the anchor */
+    if (diag_rows)
+        for (int r : *diag_rows) {
+            if (r < 0 || r >= n_rows) return GSLAM_ERR_BAD_INPUT;
+            keys.push_back((uint64_t)r * nb + (uint64_t)r);
+        }
     std::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     std::vector<int64_t> key_slot;
-    int rc = gslam_layout_from_blocks(n_rows, keys, bare, sell_window, s, &key_slot);
+    int rc = gslam_layout_from_blocks(n_rows, keys, bare, sell_window, s, &key_slot, segments);
     if (rc != GSLAM_OK) return rc;
     std::vector<int64_t> rstart(n_rows + 1, 0);
     for (uint64_t k : keys) rstart[k / nb + 1]++;

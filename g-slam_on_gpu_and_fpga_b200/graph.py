@@ -274,3 +274,61 @@ class PoseGraph:
         b = C.c_int64()
         abi.check(abi.lib().gslam_spmv_bytes(self._h, int(fp32), C.byref(b)))
         return b.value
+
+
+class PoseGraphBatch(PoseGraph):
+    """Many independent SE(2) graphs on one handle (gslam_create_se2_batch): one
+    Gauss-Newton round of every graph per `round()`, their linear solves in one
+    persistent launch with per-graph scalars. Poses of graph q are
+    `poses[offsets[q] : offsets[q] + sizes[q]]` of the concatenation."""
+
+    @classmethod
+    def from_se2_list(cls, graphs, lams, anchors=1e6, **opts) -> "PoseGraphBatch":
+        """graphs: objects with .init / .edge_i / .edge_j / .meas / .log_w (synth.CityGrid),
+        lams: one lambda per graph (or a scalar), anchors likewise."""
+        n = len(graphs)
+        lams = np.broadcast_to(np.asarray(lams, np.float64), (n,))
+        anchors = np.broadcast_to(np.asarray(anchors, np.float64), (n,))
+        keep, descs = [], (abi.SE2GraphDesc * n)()
+        for q, cg in enumerate(graphs):
+            poses = np.ascontiguousarray(cg.init, np.float64).reshape(-1, 3)
+            ei = np.ascontiguousarray(cg.edge_i, np.uint32)
+            ej = np.ascontiguousarray(cg.edge_j, np.uint32)
+            meas = np.ascontiguousarray(cg.meas, np.float64).reshape(-1, 3)
+            log_w = np.ascontiguousarray(cg.log_w, np.float64).reshape(-1, 3)
+            keep.append((poses, ei, ej, meas, log_w))
+            d = descs[q]
+            d.n_poses = poses.shape[0]
+            d.poses = abi.ptr(poses)
+            d.n_edges = ei.shape[0]
+            d.edge_i = abi.ptr(ei, C.c_uint32)
+            d.edge_j = abi.ptr(ej, C.c_uint32)
+            d.meas = abi.ptr(meas)
+            d.log_w = abi.ptr(log_w)
+            d.lam = float(lams[q])
+            d.anchor = float(anchors[q])
+        o = abi.default_opts(**opts)
+        h = C.c_void_p()
+        abi.check(abi.lib().gslam_create_se2_batch(descs, n, C.byref(o), C.byref(h)))
+        off = (C.c_uint32 * (n + 1))()
+        cnt = C.c_uint32()
+        abi.check(abi.lib().gslam_batch_layout(h, C.byref(cnt), off))
+        self = cls(h.value, int(off[n]), "se2-batch")
+        self.offsets = np.array(off[:n], np.int64)
+        self.sizes_real = np.array([k[0].shape[0] for k in keep], np.int64)
+        return self
+
+    @property
+    def n_graphs(self) -> int:
+        return len(self.offsets)
+
+    def round_all(self):
+        """One round of every graph; a RoundStats per graph."""
+        st = (abi.SolveStats * self.n_graphs)()
+        abi.check(abi.lib().gslam_batch_round(self._h, st))
+        return [RoundStats(s.iterations, s.refinements, s.reason, s.rel_residual, s.diff, s.solve_ms,
+                           s.round_ms) for s in st]
+
+    def graph_poses(self, q: int, poses=None) -> np.ndarray:
+        p = self.poses if poses is None else poses
+        return p[self.offsets[q]:self.offsets[q] + self.sizes_real[q]]

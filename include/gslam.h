@@ -222,6 +222,28 @@ int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *d_col_idx,
                            int max_iter, void *stream, gslam_solve_stats *stats);
 
 /*
+ * Batches of independent SE(2) graphs (no counterpart in the reference, which solves
+ * one graph per process and sweeps lambda with a shell loop).
+ *
+ * gslam_create_se2_batch: one handle for n_graphs graphs of any sizes, each with its
+ * own lambda and anchor. They are laid out as one block-diagonal graph, each graph's
+ * poses padded to a multiple of 32 (padding poses stay at 0). gslam_batch_layout
+ * gives the first padded pose of every graph (pose_offset[n_graphs] = total), so
+ * gslam_get_poses / gslam_set_poses work on the concatenation.
+ *
+ * gslam_batch_round: one Gauss-Newton round of every graph; the linear solves run in
+ * ONE persistent launch (block-Jacobi PCG with each graph's own alpha, beta and
+ * stopping test, tol / max_iter of the handle's options, FP64). per_graph (host,
+ * n_graphs entries, may be NULL) receives each graph's iterations, reason, relative
+ * residual and update norm diff = ||dx|| / sqrt(3 n_poses). gslam_round on a batch
+ * runs the same round and reports the largest iteration count and residual.
+ */
+int gslam_create_se2_batch(const gslam_se2_graph *graphs, uint32_t n_graphs, const gslam_opts *opts,
+                           gslam_graph **out);
+int gslam_batch_round(gslam_graph *g, gslam_solve_stats *per_graph);
+int gslam_batch_layout(gslam_graph *g, uint32_t *n_graphs, uint32_t *pose_offset);
+
+/*
  * Differentiation of a converged SE(2) graph (no counterpart in the reference, whose
  * programs only run Gauss-Newton forward).
  *

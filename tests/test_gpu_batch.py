@@ -1,0 +1,78 @@
+"""GPU tests of the batched solver (gslam_create_se2_batch / gslam_batch_round):
+graphs of uneven size with their own lambda solved in one persistent launch must
+follow the same PCG iterates, per graph, as the single-graph FP64 solver."""
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIZES = (600, 1500, 100, 2300, 37)
+LAMS = (0.1, 1.0, 0.3, 2.0, 0.5)
+
+
+@pytest.fixture(scope="module")
+def graphs():
+    synth = importlib.import_module("g-slam_on_gpu_and_fpga_b200.synth")
+    return [synth.city_grid(n, seed=10 + q) for q, n in enumerate(SIZES)]
+
+
+def single(pkg, cg, lam, **opts):
+    g = pkg.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=lam, angle_wrap=1, **opts)
+    st = g.round()
+    p = g.poses
+    g.close()
+    return st, p
+
+
+def test_batch_follows_single_graph_iterates(pkg, graphs):
+    """60 iterations, no early stop: per-graph alpha / beta must reproduce each
+    graph's own PCG iterates (only reduction order and anchor order differ)."""
+    opts = dict(tol=0.0, max_iter=60, angle_wrap=1)
+    b = pkg.PoseGraphBatch.from_se2_list(graphs, LAMS, **opts)
+    stats = b.round_all()
+    poses = b.poses
+    for q, cg in enumerate(graphs):
+        st, p = single(pkg, cg, LAMS[q], tol=0.0, max_iter=60)
+        assert stats[q].iterations == 60
+        pb = b.graph_poses(q, poses)
+        d = np.linalg.norm(pb - p) / np.linalg.norm(p - cg.init)
+        assert d < 1e-8, (q, d)
+        assert abs(stats[q].diff - st.diff) <= 1e-8 * st.diff
+    # padding poses never move
+    mask = np.ones(len(poses), bool)
+    for q in range(len(graphs)):
+        mask[b.offsets[q]:b.offsets[q] + b.sizes_real[q]] = False
+    assert np.all(poses[mask] == 0.0)
+    b.close()
+
+
+def test_batch_stops_each_graph_on_its_own(pkg, graphs):
+    opts = dict(tol=1e-8, max_iter=20000)
+    b = pkg.PoseGraphBatch.from_se2_list(graphs, LAMS, angle_wrap=1, **opts)
+    stats = b.round_all()
+    its = [s.iterations for s in stats]
+    assert len(set(its)) > 1            # the graphs need different counts
+    for q, cg in enumerate(graphs):
+        st, p = single(pkg, cg, LAMS[q], **opts)
+        assert abs(stats[q].iterations - st.iterations) <= 2, (q, stats[q].iterations, st.iterations)
+        assert stats[q].reason == 0 and stats[q].rel_residual < 1e-8
+        pb = b.graph_poses(q)
+        assert np.linalg.norm(pb - p) <= 1e-5 * np.linalg.norm(p - cg.init)
+    b.close()
+
+
+def test_lambda_sweep_in_one_batch(pkg, graphs):
+    """One graph under 8 lambdas: lambda scales every edge weight alike, so the
+    solutions agree up to the (unscaled) anchor on pose 0."""
+    lams = np.logspace(-2, 1, 8)
+    cg = graphs[0]
+    b = pkg.PoseGraphBatch.from_se2_list([cg] * len(lams), lams, tol=1e-10, max_iter=20000, angle_wrap=1)
+    stats = b.round_all()
+    poses = b.poses
+    ref = b.graph_poses(len(lams) - 1, poses)
+    for q in range(len(lams)):
+        assert stats[q].reason == 0
+        assert np.linalg.norm(b.graph_poses(q, poses) - ref) <= 1e-4 * np.linalg.norm(ref - cg.init)
+    b.close()
