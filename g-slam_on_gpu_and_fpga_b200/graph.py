@@ -316,6 +316,7 @@ class PoseGraphBatch(PoseGraph):
         self = cls(h.value, int(off[n]), "se2-batch")
         self.offsets = np.array(off[:n], np.int64)
         self.sizes_real = np.array([k[0].shape[0] for k in keep], np.int64)
+        self.init_poses = self.poses      # the concatenated initial guess (padding at 0)
         return self
 
     @property
