@@ -9,5 +9,5 @@ the GSLAM program; this package is the Python host side over that ABI:
 The directory name is not a Python identifier; import it with
 importlib.import_module("g-slam_on_gpu_and_fpga_b200").
 """
-from . import abi, build, graph, shard, synth, tune  # noqa: F401
+from . import abi, build, dense, graph, shard, synth, tune  # noqa: F401
 from .graph import PoseGraph, PoseGraphBatch, ReferenceLog, RoundStats, read_log  # noqa: F401

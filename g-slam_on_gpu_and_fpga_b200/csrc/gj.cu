@@ -1,0 +1,261 @@
+/*
+ * gj.cu — blocked Gauss-Jordan inverse of a dense FP64 matrix, the trailing update
+ * on the FP64 tensor cores.
+ *
+ * The reference's dense path (src/cpu_pcg_fp64/MatrixOps.c:29-91 `inv`, its CUDA
+ * twin src/gpu_gj_fp64/inv.cu:221-354) inverts Omega by Gauss-Jordan without
+ * pivoting and multiplies xi by the inverse; it is kept for small N as a check of
+ * the iterative solvers. Here the same elimination (no pivoting) is blocked by
+ * b = 64 columns; step k with K = [64k, 64k + 64):
+ *   U = A[:, K] (copy of the old block column), P = A[K, K]^-1 (one CTA, unblocked
+ *   in-place Gauss-Jordan in shared memory),
+ *   A[K, J] = P A[K, J]                 for J != K   (row panel)
+ *   A[I, J] = A[I, J] - U[I] A[K, J]    for I, J != K (trailing update, rank 64)
+ *   A[I, K] = -U[I] P                   for I != K,   A[K, K] = P.
+ * After the last step A holds A^-1. The row panel, trailing update and column panel
+ * are 64x64-tile GEMMs with K = 64 on mma.sync.m8n8k4 FP64 (DMMA): one CTA per
+ * output tile, both 64x64 operand tiles staged in shared memory (rows padded to 68
+ * doubles against bank conflicts), four warps of 32x32 each (4 x 4 m8n8 tiles).
+ * tcgen05 has no FP64 kind, so mma.sync is the FP64 tensor-core path on sm_100a.
+ * Operation count: 2 n^3 (the reference's unblocked version does ~4 n^3, updating
+ * the full identity side).
+ *
+ * n is padded to a multiple of 64 with an identity block (the inverse of
+ * diag(A, I) is diag(A^-1, I)).
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "gslam.h"
+#include "gslam_api_internal.h"
+
+#define GJ_B 64
+#define GJ_LD 68 /* padded leading dimension of a staged 64x64 tile */
+
+/* D = A(8x4, row) * B(4x8, col) + C, FP64: lane layout of the PTX ISA m8n8k4 .f64 shape */
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+/* sA, sB: 64x64 tiles in shared memory (row-major, ld GJ_LD); acc[4][4][2] += sA * sB
+ * for this warp's 32x32 quadrant (wm, wn) */
+__device__ __forceinline__ void tile_mma(const double *sA, const double *sB, int wm, int wn, int lane,
+                                         double (&acc)[4][4][2]) {
+    const int gid = lane >> 2, tig = lane & 3;
+#pragma unroll 4
+    for (int k = 0; k < GJ_B; k += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) a[i] = sA[(32 * wm + 8 * i + gid) * GJ_LD + k + tig];
+#pragma unroll
+        for (int j = 0; j < 4; j++) b[j] = sB[(k + tig) * GJ_LD + 32 * wn + 8 * j + gid];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+}
+
+__device__ __forceinline__ void load_tile(double *s, const double *g, int ld) {
+    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) {
+        const int r = t >> 6, c = t & 63;
+        s[r * GJ_LD + c] = g[(size_t)r * ld + c];
+    }
+}
+
+/* U = A[:, K] (n x 64, ld 64) */
+__global__ void k_gj_copy_col(int n, const double *__restrict__ A, int k0, double *__restrict__ U) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * GJ_B) return;
+    const int r = t >> 6, c = t & 63;
+    U[t] = A[(size_t)r * n + k0 + c];
+}
+
+/* P = inv(U[K, :]) by in-place Gauss-Jordan without pivoting (one CTA) */
+__global__ void k_gj_diag(const double *__restrict__ U, int k0, double *__restrict__ P) {
+    __shared__ double T[GJ_B][GJ_B + 1];
+    __shared__ double s_row[GJ_B], s_col[GJ_B];
+    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) T[t >> 6][t & 63] = U[(size_t)(k0 + (t >> 6)) * GJ_B + (t & 63)];
+    __syncthreads();
+    for (int i = 0; i < GJ_B; i++) {
+        const double p = 1.0 / T[i][i];
+        if (threadIdx.x < GJ_B) {
+            const int j = threadIdx.x;
+            s_row[j] = (j == i ? 1.0 : T[i][j]) * p; /* new pivot row */
+            s_col[j] = T[j][i];                      /* old pivot column */
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) {
+            const int r = t >> 6, c = t & 63;
+            if (r == i) T[r][c] = s_row[c];
+            else T[r][c] = (c == i ? 0.0 : T[r][c]) - s_col[r] * s_row[c];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) P[t] = T[t >> 6][t & 63];
+}
+
+/* row panel: A[K, J] = P A[K, J] for every 64-column tile J != K (one CTA per tile) */
+__global__ void __launch_bounds__(128) k_gj_row_panel(int n, double *__restrict__ A, int k0,
+                                                      const double *__restrict__ P) {
+    extern __shared__ __align__(16) double sm[];
+    double *sA = sm, *sB = sm + GJ_B * GJ_LD;
+    const int tj = blockIdx.x;
+    if (64 * tj == k0) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wm = warp >> 1, wn = warp & 1;
+    load_tile(sA, P, GJ_B);
+    load_tile(sB, A + (size_t)k0 * n + 64 * tj, n);
+    __syncthreads();
+    double acc[4][4][2] = {};
+    tile_mma(sA, sB, wm, wn, lane, acc);
+    const int gid = lane >> 2, tig = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int r = 32 * wm + 8 * i + gid, c = 32 * wn + 8 * j + 2 * tig;
+            double *dst = A + (size_t)(k0 + r) * n + 64 * tj + c;
+            dst[0] = acc[i][j][0];
+            dst[1] = acc[i][j][1];
+        }
+}
+
+/* trailing update and column panel, one CTA per 64x64 tile (I, J), I != K:
+ *   J != K: A[I, J] -= U[I] A[K, J];   J == K: A[I, K] = -U[I] P.
+ * Tile (K, K) writes P. */
+__global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A, int k0,
+                                                   const double *__restrict__ U, const double *__restrict__ P) {
+    extern __shared__ __align__(16) double sm[];
+    double *sA = sm, *sB = sm + GJ_B * GJ_LD;
+    const int ti = blockIdx.y, tj = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wm = warp >> 1, wn = warp & 1;
+    const int gid = lane >> 2, tig = lane & 3;
+    if (64 * ti == k0) {
+        if (64 * tj == k0)
+            for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x)
+                A[(size_t)(k0 + (t >> 6)) * n + k0 + (t & 63)] = P[t];
+        return;
+    }
+    const bool colp = (64 * tj == k0);
+    load_tile(sA, U + (size_t)(64 * ti) * GJ_B, GJ_B);
+    load_tile(sB, colp ? P : A + (size_t)k0 * n + 64 * tj, colp ? GJ_B : n);
+    __syncthreads();
+    double acc[4][4][2] = {};
+    tile_mma(sA, sB, wm, wn, lane, acc);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int r = 32 * wm + 8 * i + gid, c = 32 * wn + 8 * j + 2 * tig;
+            double *dst = A + (size_t)(64 * ti + r) * n + 64 * tj + c;
+            if (colp) {
+                dst[0] = -acc[i][j][0];
+                dst[1] = -acc[i][j][1];
+            } else {
+                dst[0] = dst[0] - acc[i][j][0];
+                dst[1] = dst[1] - acc[i][j][1];
+            }
+        }
+}
+
+/* pad: B (m x m, m = n rounded up to 64) = diag(A, I) */
+__global__ void k_gj_pad(int n, int m, const double *__restrict__ A, int lda, double *__restrict__ B) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)m * m) return;
+    const int r = (int)(t / m), c = (int)(t % m);
+    B[t] = (r < n && c < n) ? A[(size_t)r * lda + c] : (r == c ? 1.0 : 0.0);
+}
+
+__global__ void k_gj_unpad(int n, int m, const double *__restrict__ B, double *__restrict__ A, int lda) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * n) return;
+    const int r = (int)(t / n), c = (int)(t % n);
+    A[(size_t)r * lda + c] = B[(size_t)r * m + c];
+}
+
+/* y = A x, one warp per row (A m x m, row-major), summed in a fixed order */
+__global__ void k_gemv(int m, const double *__restrict__ A, const double *__restrict__ x, double *__restrict__ y) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= m) return;
+    double s = 0.0;
+    for (int c = lane; c < m; c += 32) s = s + A[(size_t)row * m + c] * x[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) y[row] = s;
+}
+
+static int gj_run(int m, double *d_a, cudaStream_t st, double *scratch) {
+    /* scratch: U (m x 64) then P (64 x 64) */
+    double *U = scratch, *P = scratch + (size_t)m * GJ_B;
+    const size_t smem = 2 * GJ_B * GJ_LD * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gj_row_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    const int nt = m / GJ_B;
+    for (int k = 0; k < nt; k++) {
+        const int k0 = GJ_B * k;
+        k_gj_copy_col<<<(m * GJ_B + 255) / 256, 256, 0, st>>>(m, d_a, k0, U);
+        k_gj_diag<<<1, 1024, 0, st>>>(U, k0, P);
+        k_gj_row_panel<<<nt, 128, smem, st>>>(m, d_a, k0, P);
+        k_gj_update<<<dim3(nt, nt), 128, smem, st>>>(m, d_a, k0, U, P);
+    }
+    return cudaGetLastError() == cudaSuccess ? GSLAM_OK : GSLAM_ERR_CUDA;
+}
+
+int gslam_gj_inverse(int n, double *d_a, int lda, void *stream, float *ms) {
+    if (n <= 0 || !d_a || lda < n) { gslam_set_last_error("bad dense matrix"); return GSLAM_ERR_BAD_INPUT; }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int m = (n + GJ_B - 1) / GJ_B * GJ_B;
+    double *B = nullptr, *scratch = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = GSLAM_ERR_CUDA;
+    if (cudaMalloc(&B, (size_t)m * m * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&scratch, ((size_t)m * GJ_B + GJ_B * GJ_B) * sizeof(double)) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        gslam_set_last_error("cudaMalloc failed (dense inverse)");
+        goto done;
+    }
+    k_gj_pad<<<(unsigned)(((size_t)m * m + 255) / 256), 256, 0, st>>>(n, m, d_a, lda, B);
+    cudaEventRecord(e0, st);
+    rc = gj_run(m, B, st, scratch);
+    cudaEventRecord(e1, st);
+    if (rc == GSLAM_OK) {
+        k_gj_unpad<<<(unsigned)(((size_t)n * n + 255) / 256), 256, 0, st>>>(n, m, B, d_a, lda);
+        if (cudaStreamSynchronize(st) != cudaSuccess) { rc = GSLAM_ERR_CUDA; gslam_set_last_error("dense inverse failed"); }
+        else if (ms) cudaEventElapsedTime(ms, e0, e1);
+    } else {
+        gslam_set_last_error("dense inverse launch failed");
+    }
+done:
+    if (B) cudaFree(B);
+    if (scratch) cudaFree(scratch);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return rc;
+}
+
+int gslam_gj_solve(int n, const double *d_a, int lda, const double *d_b, double *d_x, void *stream, float *ms) {
+    if (n <= 0 || !d_a || !d_b || !d_x || lda < n) { gslam_set_last_error("bad dense system"); return GSLAM_ERR_BAD_INPUT; }
+    cudaStream_t st = (cudaStream_t)stream;
+    double *A = nullptr;
+    if (cudaMalloc(&A, (size_t)n * n * sizeof(double)) != cudaSuccess) {
+        gslam_set_last_error("cudaMalloc failed (dense solve)");
+        return GSLAM_ERR_CUDA;
+    }
+    cudaMemcpy2DAsync(A, n * sizeof(double), d_a, lda * sizeof(double), n * sizeof(double), n,
+                      cudaMemcpyDeviceToDevice, st);
+    int rc = gslam_gj_inverse(n, A, n, stream, ms);
+    if (rc == GSLAM_OK) {
+        k_gemv<<<(n * 32 + 255) / 256, 256, 0, st>>>(n, A, d_b, d_x);
+        if (cudaStreamSynchronize(st) != cudaSuccess) { rc = GSLAM_ERR_CUDA; gslam_set_last_error("dense solve failed"); }
+    }
+    cudaFree(A);
+    return rc;
+}

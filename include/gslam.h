@@ -244,6 +244,20 @@ int gslam_batch_round(gslam_graph *g, gslam_solve_stats *per_graph);
 int gslam_batch_layout(gslam_graph *g, uint32_t *n_graphs, uint32_t *pose_offset);
 
 /*
+ * Dense Gauss-Jordan inverse / solve, replacing the reference's dense check path
+ * (inv: src/cpu_pcg_fp64/MatrixOps.c:29-91 and its CUDA twin
+ * src/gpu_gj_fp64/inv.cu:221-354; Omega^-1 then Omega^-1 xi): elimination without
+ * pivoting, blocked by 64 columns, trailing updates on the FP64 tensor cores.
+ * Matrices are row-major device memory with leading dimension lda; stream is a
+ * cudaStream_t (NULL = legacy default stream). gslam_gj_inverse overwrites d_a with
+ * its inverse; gslam_gj_solve leaves d_a unchanged and writes x = A^-1 b to d_x.
+ * ms (may be NULL) receives the device time of the elimination. Both allocate their
+ * scratch (an n x n copy padded to a multiple of 64) and synchronize the stream.
+ */
+int gslam_gj_inverse(int n, double *d_a, int lda, void *stream, float *ms);
+int gslam_gj_solve(int n, const double *d_a, int lda, const double *d_b, double *d_x, void *stream, float *ms);
+
+/*
  * Differentiation of a converged SE(2) graph (no counterpart in the reference, whose
  * programs only run Gauss-Newton forward).
  *
