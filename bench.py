@@ -323,6 +323,20 @@ def batch_sample(G, torch, rounds, world, rank, dist):
             "dtype": "f64", "config": "48 graphs N~logU[500, 20000] + one N=5000 graph x 16 lambdas in [0.01, 10]"}
 
 
+def spmv_sample(g, peaks):
+    """Standalone SpMV from HBM: one launch multiplies many copies of the N=100k matrix
+    (more bytes than three L2s), so every value is read from HBM; achieved = algorithmic
+    bytes (values, columns, slice pointers, x gathered once, y written) / time."""
+    out = {}
+    for name, fp32, copies in (("fp64", False, 16), ("fp32", True, 32)):
+        ms = g.spmv_bench(fp32, reps=10, n_copies=copies)
+        nbytes = g.spmv_bytes(fp32)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": round(ms, 5), "algorithmic_bytes": nbytes, "achieved_gbs": round(gbs, 1),
+                     "frac": round(gbs / peaks["hbm_gbs"], 4), "copies_per_launch": copies}
+    return out
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -412,6 +426,7 @@ def run_ours(args):
         line["cpu_baseline"] = cpu
     if not args.no_batch:
         line["batch"] = batch_sample(G, torch, 3, world, rank, dist)
+    line["spmv_hbm"] = spmv_sample(results["fp64"]["g"], peaks)
     for arm in results.values():
         arm["g"].close()
     if rank == 0:
@@ -476,6 +491,12 @@ def run_ncu_case(args):
                              tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=prec)
     g.linearise()
     g.assemble()
+    if args.ncu_case == "spmv":
+        # two launches (warm-up + one timed) of 16 FP64 copies of the matrix
+        ms = g.spmv_bench(False, reps=1, n_copies=16)
+        print(f"spmv: {ms:.4f} ms per matrix", flush=True)
+        g.close()
+        return
     for iters in (50, 250):
         g.set_opts(precision=prec, tol=0.0, max_iter=iters, inner_max_iter=iters)
         st = g.solve()
@@ -492,7 +513,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-graph batched-solve sample")
-    ap.add_argument("--ncu-case", choices=["fp64", "mixed"], default=None,
+    ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv"], default=None,
                     help="run only two short solves of the workload (for ncu captures)")
     args = ap.parse_args()
     if args.ncu_case:

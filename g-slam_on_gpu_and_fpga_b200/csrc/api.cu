@@ -801,57 +801,78 @@ int gslam_spmv_bench(gslam_graph *g, int prec, int reps, int n_copies, float *ms
     if (prec == 1) {
         int rc = gslam_layout_ensure_fp32(&g->L, g->st);
         if (rc != GSLAM_OK) return rc;
+        if (!g->L.val32_fresh) {
+            launch_val_to_f32(g->st, 9 * g->L.n_slots, g->L.val, g->L.val32);
+            g->L.val32_fresh = true;
+        }
     }
     DevLayout &L = g->L;
     const size_t nv = 9 * (size_t)L.n_slots;
     const size_t esz = prec == 1 ? sizeof(float) : sizeof(double);
-    std::vector<void *> copies;
-    copies.push_back(prec == 1 ? (void *)L.val32 : (void *)L.val);
-    int rc = GSLAM_OK;
-    for (int c = 1; c < n_copies; c++) {
-        void *q = nullptr;
-        if (cudaMalloc(&q, nv * esz) != cudaSuccess) { rc = GSLAM_ERR_CUDA; break; }
-        copies.push_back(q);
-        cudaMemcpyAsync(q, copies[0], nv * esz, cudaMemcpyDeviceToDevice, g->st);
-    }
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    const size_t ny = 4 * 32 * (size_t)L.n_slices;
+    /* n_copies value arrays back to back (the matrix repeated) and one result per copy:
+     * with n_copies large enough the stream exceeds L2 and every launch reads HBM */
+    char *vals = nullptr, *ys = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
     float t = 0.f;
+    int rc = GSLAM_OK;
+    if (cudaMalloc(&vals, nv * esz * n_copies) != cudaSuccess || cudaMalloc(&ys, ny * esz * n_copies) != cudaSuccess) {
+        g_last_error = "spmv bench: cudaMalloc failed";
+        rc = GSLAM_ERR_CUDA;
+    }
     if (rc == GSLAM_OK) {
-        cudaStreamSynchronize(g->st);
-        cudaError_t e = cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal);
-        for (int i = 0; i < reps && e == cudaSuccess; i++) {
-            const void *v = copies[i % copies.size()];
+        const void *src = prec == 1 ? (const void *)L.val32 : (const void *)L.val;
+        for (int c = 0; c < n_copies; c++)
+            cudaMemcpyAsync(vals + c * nv * esz, src, nv * esz, cudaMemcpyDeviceToDevice, g->st);
+        auto launch = [&]() {
             if (prec == 1)
-                launch_spmv32(g->st, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col,
-                              (const float *)v, L.f[3], L.f[5]);
+                launch_spmv_multi32(g->st, n_copies, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col,
+                                    (const float *)vals, (int64_t)nv, L.f[3], (float *)ys, (int64_t)ny);
             else
-                launch_spmv64(g->st, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col,
-                              (const double *)v, L.p4a, L.q4);
-        }
-        cudaError_t e2 = cudaStreamEndCapture(g->st, &graph);
-        if (e == cudaSuccess) e = e2;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-        if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->st);      /* warm-up replay */
-        if (e == cudaSuccess) e = cudaEventCreate(&a);
+                launch_spmv_multi64(g->st, n_copies, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col,
+                                    (const double *)vals, (int64_t)nv, L.p4a, (double *)ys, (int64_t)ny);
+        };
+        launch(); /* warm-up */
+        cudaError_t e = cudaEventCreate(&a);
         if (e == cudaSuccess) e = cudaEventCreate(&b);
         if (e == cudaSuccess) e = cudaEventRecord(a, g->st);
-        if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->st);
+        for (int i = 0; i < reps && e == cudaSuccess; i++) launch();
         if (e == cudaSuccess) e = cudaEventRecord(b, g->st);
         if (e == cudaSuccess) e = cudaEventSynchronize(b);
         if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+        if (e == cudaSuccess) e = cudaGetLastError();
         if (e != cudaSuccess) {
             g_last_error = std::string("spmv bench: ") + cudaGetErrorString(e);
             rc = GSLAM_ERR_CUDA;
         }
+        /* self-check: copy 0's result against the single-matrix SpMV kernel (same
+         * summation order, so equal bit for bit) */
+        if (rc == GSLAM_OK) {
+            if (prec == 1) launch_spmv32(g->st, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col, L.val32,
+                                         L.f[3], L.f[5]);
+            else launch_spmv64(g->st, g->n_poses, L.n_slices, L.slice_ptr, L.row_len, L.col, L.val, L.p4a, L.q4);
+            std::vector<char> y0(ny * esz), y1(ny * esz);
+            cudaMemcpyAsync(y0.data(), ys, ny * esz, cudaMemcpyDeviceToHost, g->st);
+            cudaMemcpyAsync(y1.data(), prec == 1 ? (const void *)L.f[5] : (const void *)L.q4, ny * esz,
+                            cudaMemcpyDeviceToHost, g->st);
+            if (cudaStreamSynchronize(g->st) != cudaSuccess) { g_last_error = "spmv bench: check failed"; rc = GSLAM_ERR_CUDA; }
+            else {
+                /* components 0..2 of the real rows (padding is never written) */
+                bool same = true;
+                for (int r = 0; r < g->n_poses && same; r++)
+                    same = memcmp(y0.data() + 4 * r * esz, y1.data() + 4 * r * esz, 3 * esz) == 0;
+                if (!same) {
+                    g_last_error = "spmv bench: the many-matrix kernel disagrees with the single-matrix one";
+                    rc = GSLAM_ERR_CUDA;
+                }
+            }
+        }
     }
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    for (size_t c = 1; c < copies.size(); c++) cudaFree(copies[c]);
-    if (rc == GSLAM_OK) *ms = t / reps;
+    if (vals) cudaFree(vals);
+    if (ys) cudaFree(ys);
+    if (rc == GSLAM_OK) *ms = t / reps / n_copies;
     return rc;
 }
 

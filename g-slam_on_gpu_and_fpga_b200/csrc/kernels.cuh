@@ -85,6 +85,14 @@ struct PcgParams {
     int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
 };
 
+/* SpMV of n_copies matrices sharing one block pattern, in one launch (pcg.cu). */
+void launch_spmv_multi64(cudaStream_t st, int n_copies, int n_rows, int n_slices, const int64_t *slice_ptr,
+                         const int *row_len, const int *col, const double *val, int64_t stride,
+                         const double *x4, double *y4, int64_t ystride);
+void launch_spmv_multi32(cudaStream_t st, int n_copies, int n_rows, int n_slices, const int64_t *slice_ptr,
+                         const int *row_len, const int *col, const float *val, int64_t stride,
+                         const float *x4, float *y4, int64_t ystride);
+
 /* Batched solver (batch.cu): per-graph scalars over a block-diagonal system. */
 struct BatchParams {
     int n_graphs;

@@ -251,6 +251,73 @@ int pcg_max_grid(int precision, int block, int device) {
     return std::min(per_sm, per_sm2) * n_sm;
 }
 
+/*
+ * Many matrices with one block pattern in one launch (the L2-busting SpMV
+ * measurement): warp w handles slice w % n_slices of copy w / n_slices, whose values
+ * start at val + copy * stride and whose result goes to y4 + copy * ystride.
+ */
+template <typename T>
+__global__ void k_spmv_multi(int n_copies, int n_rows, int n_slices, const int64_t *__restrict__ slice_ptr,
+                             const int *__restrict__ row_len, const int *__restrict__ col,
+                             const T *__restrict__ val, int64_t stride, const T *__restrict__ x4,
+                             T *__restrict__ y4, int64_t ystride) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t copy = gw / n_slices;
+    const int s = (int)(gw - copy * n_slices);
+    if (copy >= n_copies) return;
+    const int row = 32 * s + lane;
+    if (row >= n_rows) return;
+    const int len = __ldg(row_len + row);
+    const int64_t sb = __ldg(slice_ptr + s);
+    const T *vb = val + copy * stride + 9 * sb + lane;
+    const int *cb = col + sb + lane;
+    T q0 = 0, q1 = 0, q2 = 0;
+    int j = 0;
+    for (; j + 1 < len; j += 2) {
+        const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
+        const T *p0 = x4 + 4 * (size_t)c0, *p1 = x4 + 4 * (size_t)c1;
+        const T a0 = __ldg(p0), a1 = __ldg(p0 + 1), a2 = __ldg(p0 + 2);
+        const T b0 = __ldg(p1), b1 = __ldg(p1 + 1), b2 = __ldg(p1 + 2);
+        const T *v0 = vb + 288 * j, *v1 = v0 + 288;
+        q0 = q0 + __ldg(v0) * a0;       q0 = q0 + __ldg(v0 + 32) * a1;  q0 = q0 + __ldg(v0 + 64) * a2;
+        q1 = q1 + __ldg(v0 + 96) * a0;  q1 = q1 + __ldg(v0 + 128) * a1; q1 = q1 + __ldg(v0 + 160) * a2;
+        q2 = q2 + __ldg(v0 + 192) * a0; q2 = q2 + __ldg(v0 + 224) * a1; q2 = q2 + __ldg(v0 + 256) * a2;
+        q0 = q0 + __ldg(v1) * b0;       q0 = q0 + __ldg(v1 + 32) * b1;  q0 = q0 + __ldg(v1 + 64) * b2;
+        q1 = q1 + __ldg(v1 + 96) * b0;  q1 = q1 + __ldg(v1 + 128) * b1; q1 = q1 + __ldg(v1 + 160) * b2;
+        q2 = q2 + __ldg(v1 + 192) * b0; q2 = q2 + __ldg(v1 + 224) * b1; q2 = q2 + __ldg(v1 + 256) * b2;
+    }
+    if (j < len) {
+        const int c0 = __ldg(cb + 32 * j);
+        const T *p0 = x4 + 4 * (size_t)c0;
+        const T a0 = __ldg(p0), a1 = __ldg(p0 + 1), a2 = __ldg(p0 + 2);
+        const T *v0 = vb + 288 * j;
+        q0 = q0 + __ldg(v0) * a0;       q0 = q0 + __ldg(v0 + 32) * a1;  q0 = q0 + __ldg(v0 + 64) * a2;
+        q1 = q1 + __ldg(v0 + 96) * a0;  q1 = q1 + __ldg(v0 + 128) * a1; q1 = q1 + __ldg(v0 + 160) * a2;
+        q2 = q2 + __ldg(v0 + 192) * a0; q2 = q2 + __ldg(v0 + 224) * a1; q2 = q2 + __ldg(v0 + 256) * a2;
+    }
+    T *y = y4 + copy * ystride + 4 * (size_t)row;
+    y[0] = q0;
+    y[1] = q1;
+    y[2] = q2;
+}
+
+void launch_spmv_multi64(cudaStream_t st, int n_copies, int n_rows, int n_slices, const int64_t *slice_ptr,
+                         const int *row_len, const int *col, const double *val, int64_t stride,
+                         const double *x4, double *y4, int64_t ystride) {
+    const int64_t nthreads = 32 * (int64_t)n_slices * n_copies;
+    k_spmv_multi<double><<<(unsigned)((nthreads + 255) / 256), 256, 0, st>>>(
+        n_copies, n_rows, n_slices, slice_ptr, row_len, col, val, stride, x4, y4, ystride);
+}
+
+void launch_spmv_multi32(cudaStream_t st, int n_copies, int n_rows, int n_slices, const int64_t *slice_ptr,
+                         const int *row_len, const int *col, const float *val, int64_t stride,
+                         const float *x4, float *y4, int64_t ystride) {
+    const int64_t nthreads = 32 * (int64_t)n_slices * n_copies;
+    k_spmv_multi<float><<<(unsigned)((nthreads + 255) / 256), 256, 0, st>>>(
+        n_copies, n_rows, n_slices, slice_ptr, row_len, col, val, stride, x4, y4, ystride);
+}
+
 void launch_spmv64(cudaStream_t st, int n_rows, int n_slices, const int64_t *slice_ptr,
                    const int *row_len, const int *col, const double *val, const double *x4,
                    double *y4) {

@@ -161,10 +161,11 @@ int gslam_get_diag_inv(gslam_graph *g, double *dinv);
 /* y = Omega x on device pointers in original order [3N] (FP64, row sums in column order). */
 int gslam_spmv(gslam_graph *g, const double *d_x, double *d_y);
 /*
- * Times `reps` FP64 (prec 0) or FP32 (prec 1) SpMVs y = Omega x, replayed from one CUDA
- * graph; *ms = mean device milliseconds per SpMV. n_copies > 1 rotates through that many
- * copies of the matrix values (allocated for the call) so consecutive SpMVs read different
- * memory: with n_copies * bytes above three L2 sizes every SpMV streams from HBM.
+ * Times FP64 (prec 0) or FP32 (prec 1) SpMVs y = Omega x: each of `reps` launches
+ * multiplies n_copies copies of the matrix values (allocated for the call, back to
+ * back, one result vector each) by the same x; *ms = mean device milliseconds per
+ * matrix. With n_copies * matrix bytes above three L2 sizes every launch streams
+ * its values from HBM.
  */
 int gslam_spmv_bench(gslam_graph *g, int prec, int reps, int n_copies, float *ms);
 /* Algorithmic bytes of one SpMV: values, column indices, x read once, y written once. */
