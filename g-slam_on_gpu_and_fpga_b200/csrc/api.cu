@@ -393,6 +393,24 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
         g_last_error = "solver barrier wait timed out";
         return GSLAM_ERR_DEVICE_TIMEOUT;
     }
+    if (mixed && h_res->reason == GSLAM_STOP_STAGNATION) {
+        /* the FP32 inner solve cannot resolve this system: solve it in FP64 (from x = 0;
+         * the right-hand side is untouched) and report both */
+        const int refs = h_res->refinements, its = h_res->iterations;
+        gslam_opts o64 = o;
+        o64.precision = GSLAM_PREC_FP64;
+        gslam_solve_stats s64;
+        memset(&s64, 0, sizeof s64);
+        int rc = gslam_layout_solve(L, st, o64, h_res, &s64);
+        if (stats) {
+            stats->solve_ms += s64.solve_ms;
+            stats->iterations = its + s64.iterations;
+            stats->refinements = -refs;
+            stats->reason = s64.reason;
+            stats->rel_residual = s64.rel_residual;
+        }
+        return rc;
+    }
     return GSLAM_OK;
 }
 

@@ -38,7 +38,9 @@
  * shared memory only.
  *
  * Outer step: x += d (FP64), grid barrier, r = xi - Omega x with the FP64 matrix,
- * ||r|| -> stop at tol * ||xi||, else restart the inner solve from r.
+ * ||r|| -> stop at tol * ||xi||, else restart the inner solve from r; a step that
+ * does not halve ||r|| ends the solve with GSLAM_STOP_STAGNATION (the host then
+ * solves in FP64).
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -179,7 +181,8 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
         return;
     }
     if (threadIdx.x == 0) {
-        s_sc[3] = P.tol_rel * sqrt(bb[0]);
+        const double tol = P.tol_rel * sqrt(bb[0]);
+        s_sc[3] = tol * tol;     /* compared with rho = r.r, so no square root per iteration */
         s_sc[4] = sqrt(bb[0]);
     }
 
@@ -236,41 +239,55 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
             p = axpy_f(beta, p, z);
             if (k > 0) d = axpy_f(alpha, p, d);
             step_zv(z, u, v, alpha, beta, z, v);
-            if (mine) stf3(sz, row - row0, z);
+            if (mine) {
+                stf3(sz, row - row0, z);
+                /* z_k and v_{k-1} are final here: publish them now, so only u_k's stores
+                 * are still in flight when the CTA arrives at the barrier */
+                stf3(PUB_Z(pw), row, z);
+                stf3(PUB_V(pw), row, v);
+            }
             __syncthreads();
             /* w_k = A z_k from shared memory, u_k = D^-1 w_k */
             double part[3] = { 0.0, 0.0, 0.0 };
+            float q0 = 0.f, q1 = 0.f, q2 = 0.f;
             if (mine) {
-                float q0 = 0.f, q1 = 0.f, q2 = 0.f;
                 const int *cb = scol + lslot + lane;
+                const int jend = len;
+                const int jsm = j_sm;
                 int j = 0;
                 /* four blocks at a time: their column and z loads are in flight together
                  * (a row's blocks are still added in ascending column order) */
                 const float *sv0 = sval + 9 * lslot + lane;
-                for (; j + 3 < j_sm; j += 4) {
+                /* the diagonal block's z is this thread's own (no shared-memory load) */
+                const int lrow = row - row0;
+                for (; j + 3 < jsm; j += 4) {
                     const int c0 = cb[32 * j], c1 = cb[32 * (j + 1)], c2 = cb[32 * (j + 2)], c3 = cb[32 * (j + 3)];
-                    const F3 z0 = ldf3(sz, c0), z1 = ldf3(sz, c1), z2 = ldf3(sz, c2), z3 = ldf3(sz, c3);
+                    const F3 z0 = c0 == lrow ? z : ldf3(sz, c0), z1 = c1 == lrow ? z : ldf3(sz, c1);
+                    const F3 z2 = c2 == lrow ? z : ldf3(sz, c2), z3 = c3 == lrow ? z : ldf3(sz, c3);
                     blk_acc_f(sv0 + 288 * j, z0, q0, q1, q2);
                     blk_acc_f(sv0 + 288 * (j + 1), z1, q0, q1, q2);
                     blk_acc_f(sv0 + 288 * (j + 2), z2, q0, q1, q2);
                     blk_acc_f(sv0 + 288 * (j + 3), z3, q0, q1, q2);
                 }
-                for (; j < j_sm; j++) blk_acc_f(sv0 + 288 * j, ldf3(sz, cb[32 * j]), q0, q1, q2);
-                if (j < len) {
+                for (; j < jsm; j++) {
+                    const int c0 = cb[32 * j];
+                    blk_acc_f(sv0 + 288 * j, c0 == lrow ? z : ldf3(sz, c0), q0, q1, q2);
+                }
+                if (j < jend) {
                     /* blocks beyond the shared-memory share: values from L2 */
                     const float *gv = P.val32 + 9 * __ldg(P.slice_ptr + s) + lane;
-                    for (; j < len; j++) blk_acc_f(gv + 288 * j, ldf3(sz, cb[32 * j]), q0, q1, q2);
+                    for (; j < jend; j++) blk_acc_f(gv + 288 * j, ldf3(sz, cb[32 * j]), q0, q1, q2);
                 }
+            }
+            if (mine) {
                 w = F3{ q0, q1, q2 };
                 u = dinv_apply_f(sdinv + 288 * warp + lane, w); /* own row's D^-1 (stride 32) */
                 const double r0 = r.a, r1 = r.b, r2 = r.c, z0 = z.a, z1 = z.b, z2 = z.c;
                 part[0] = r0 * z0 + r1 * z1 + r2 * z2;                            /* gamma */
                 part[1] = (double)w.a * z0 + (double)w.b * z1 + (double)w.c * z2; /* delta */
                 part[2] = r0 * r0 + r1 * r1 + r2 * r2;                            /* rho */
-                /* publish z_k, u_k, v_{k-1} for iteration k + 1 */
-                stf3(PUB_Z(pw), row, z);
+                /* publish u_k for iteration k + 1 (z_k and v_{k-1} went out before the SpMV) */
                 stf3(PUB_U(pw), row, u);
-                stf3(PUB_V(pw), row, v);
             }
             if (!grid_reduce_arrive<3, BS>(part, P.partials, epoch, P.gs, P.spin_limit, s_red, &s_ok)) {
                 timed_out = true;
@@ -282,27 +299,31 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
             total++;
             k++;
             if (threadIdx.x == 0) {
+                /* alpha_k = gamma / (delta - beta_k gamma / alpha_{k-1}) = gamma g / (delta g - gamma^2)
+                 * with g = gamma_{k-1} alpha_{k-1}: the products in FP64 (the cancellation
+                 * happens there), the two quotients in FP32 (they are used as FP32 and
+                 * are the recurrence's state: alpha_{k-1} is the value the vectors used) */
                 const double gamma = s_bc[0], delta = s_bc[1], rho = s_bc[2];
                 if (k == 1) s_sc[2] = rho;
-                double a, bt;
-                /* alpha_k = gamma / (delta - beta_k gamma / alpha_{k-1}) rewritten with
-                 * g = gamma_{k-1} alpha_{k-1}, so one division is on the critical path
-                 * (beta's runs beside it) */
-                if (k == 1) { bt = 0.0; a = gamma / delta; }
+                double num, den;
+                float bt;
+                if (k == 1) { bt = 0.f; num = gamma; den = delta; }
                 else {
                     const double g = s_sc[0] * s_sc[1];
-                    bt = gamma / s_sc[0];
-                    a = (gamma * g) / (delta * g - gamma * gamma);
+                    bt = (float)gamma / (float)s_sc[0];
+                    num = gamma * g;
+                    den = delta * g - gamma * gamma;
                 }
+                const float a = (float)num / (float)den;
                 int flag = 0;
-                if (!(delta != 0.0) || !(a == a)) flag = 2;
+                if (!(delta != 0.0) || !(den != 0.0) || !(a == a) || isinf(a)) flag = 2;
                 else if (rho <= P.inner_tol * P.inner_tol * s_sc[2] || k >= P.inner_max_iter ||
-                         total >= P.max_iter || sqrt(rho) < s_sc[3])
+                         total >= P.max_iter || rho < s_sc[3])
                     flag = 1;
                 s_sc[0] = gamma;
-                s_sc[1] = a;
-                s_ab[0] = (float)a;
-                s_ab[1] = (float)bt;
+                s_sc[1] = (double)a;
+                s_ab[0] = a;
+                s_ab[1] = bt;
                 s_flag = flag;
             }
             __syncthreads();
@@ -337,8 +358,16 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
             timed_out = true;
             break;
         }
+        const double rnorm_prev = rnorm;
         rnorm = sqrt(rr[0]);
         if (reason == GSLAM_STOP_PQ_ZERO) break;
+        /* iterative refinement must shrink the true residual; when a step gains less than a
+         * factor 2 the FP32 inner solve cannot resolve this system (cond x eps32 >> 1) */
+        if (rnorm >= P.tol_rel * s_sc[4] && total < P.max_iter && outer < P.max_refine &&
+            rnorm > 0.5 * rnorm_prev) {
+            reason = GSLAM_STOP_STAGNATION;
+            break;
+        }
     }
 #undef PUB_Z
 #undef PUB_U

@@ -45,6 +45,9 @@ extern "C" {
 #define GSLAM_STOP_MAXIT 1   /* iteration cap reached */
 #define GSLAM_STOP_PQ_ZERO 2 /* p.Ap == 0 (MatrixOps.c:357) */
 #define GSLAM_STOP_TIMEOUT 3 /* device barrier wait gave up */
+#define GSLAM_STOP_STAGNATION 4 /* mixed: a refinement step reduced ||r|| by less than half (the
+                                 * FP32 inner solve cannot resolve this system); the library then
+                                 * solves in FP64 and reports that solve's reason */
 
 typedef struct gslam_opts {
     int precision;        /* GSLAM_PREC_*; default FP64 */
@@ -66,7 +69,8 @@ typedef struct gslam_opts {
 
 typedef struct gslam_solve_stats {
     int iterations;       /* PCG iterations (mixed: total inner iterations) */
-    int refinements;      /* mixed: outer FP64 steps; FP64: 0 */
+    int refinements;      /* mixed: outer FP64 steps (negative: the FP64 solver finished the
+                           * solve after the mixed one stagnated at -refinements steps); FP64: 0 */
     int reason;           /* GSLAM_STOP_* */
     double rel_residual;  /* ||b - A x|| / ||b|| as tracked by the solver */
     double diff;          /* ||dx|| / sqrt(dim) (GSLAM.c:104-105) */
