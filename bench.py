@@ -337,6 +337,45 @@ def spmv_sample(g, peaks):
     return out
 
 
+def c2_sample(G, rounds=50):
+    """Per-round pose and residual error against the FP64 CPU oracle on the 7,120-pose
+    walk with denser revisits (up to 6 closures within 3 m, ~2% of poses closing more
+    than 1,000 steps back), lambda 1.0, the reference's PCG settings, FP64 and mixed."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    cg = G.synth.city_grid(7120, seed=2, k_closures=6, radius=3.0, far_fraction=0.02)
+    lam = 1.0
+    dim = 3 * cg.n_poses
+    p = cg.init.copy()
+    ref = []
+    t0 = time.perf_counter()
+    for _ in range(rounds):
+        blocks, _ = O.se2_linearise(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam)
+        rp, ci, va, xi = O.csr_build_anchor(dim, cg.edge_i, cg.edge_j, blocks, 1e6)
+        dx, _, _ = O.pcg(rp, ci, va, xi, tol=TOL, max_iter=MAX_ITER)
+        p = p + dx.reshape(-1, 3)
+        p[:, 2] = (p[:, 2] + np.pi) % (2 * np.pi) - np.pi
+        ref.append(p.copy())
+    cpu_s = time.perf_counter() - t0
+    out = {"config": "N=7120, K=6 within 3 m, 2% far closures, lambda 1.0, 50 rounds, tol 1e-6 / 500",
+           "oracle_seconds": round(cpu_s, 2)}
+    for name, prec in (("fp64", G.abi.PREC_FP64), ("mixed", G.abi.PREC_MIXED)):
+        g = G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=lam,
+                                 tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=prec)
+        errs, res = [], []
+        for k in range(rounds):
+            st = g.round()
+            errs.append(pose_err_rel(g.poses, ref[k]))
+            res.append(st.rel_residual)
+        g.close()
+        out[name] = {"pose_err_rel_per_round": [float(f"{e:.3e}") for e in errs],
+                     "rel_residual_per_round": [float(f"{r:.3e}") for r in res],
+                     "max_pose_err_rel": max(errs)}
+    return out
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_env()
@@ -427,6 +466,8 @@ def run_ours(args):
     if not args.no_batch:
         line["batch"] = batch_sample(G, torch, 3, world, rank, dist)
     line["spmv_hbm"] = spmv_sample(results["fp64"]["g"], peaks)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["per_round_vs_oracle"] = c2_sample(G)
     for arm in results.values():
         arm["g"].close()
     if rank == 0:

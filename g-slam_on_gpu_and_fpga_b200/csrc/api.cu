@@ -229,7 +229,7 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             /* CTA-local column indices (own rows first, then the CTA's halo) and halo lists */
             std::vector<int> lcol(S.n_slots, 0), hptr(rgrid + 1, 0), hrows;
             int64_t p_cap = 0;
-            int sl_max = 0;
+            int sl_max = 0, h_max = 0;
             for (int i = 0; i < rgrid; i++) {
                 const int row0 = 32 * cs[i], row1 = 32 * cs[i + 1], nloc = row1 - row0;
                 const int64_t a0 = S.slice_ptr[cs[i]], a1 = S.slice_ptr[cs[i + 1]];
@@ -250,6 +250,7 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 hrows.insert(hrows.end(), rem.begin(), rem.end());
                 p_cap = std::max<int64_t>(p_cap, nloc + (int64_t)rem.size());
                 sl_max = std::max(sl_max, cs[i + 1] - cs[i]);
+                h_max = std::max(h_max, (int)rem.size());
             }
             /* FP64: values | local columns | staged p (32 B per own or halo row) */
             const int64_t p_bytes = 32 * p_cap;
@@ -261,16 +262,19 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 L->smem_bytes = (size_t)(L->smem_p_off + p_bytes);
             }
             /* mixed: FP32 values | local columns | D^-1 of own rows (2304 B per slice) |
-             * z of own and halo rows (16 B each) */
+             * z of own and halo rows (16 B each) | u, v of the first `block` halo rows
+             * (32 B each, copied in asynchronously) */
             const int64_t z_bytes = (16 * p_cap + 127) / 128 * 128;
-            const int64_t fixed = col_bytes + 2304 * (int64_t)sl_max + z_bytes;
+            const int64_t stage_bytes = (32 * (int64_t)std::min(h_max, block) + 127) / 128 * 128;
+            const int64_t fixed = col_bytes + 2304 * (int64_t)sl_max + z_bytes + stage_bytes;
             const int64_t cap32 = ((int64_t)GSLAM_RES_SMEM_MAX - fixed) / 4 / 288 * 288;
             if (cap32 >= 0) {
                 L->mixed_ok = true;
                 L->mixed_val_cap = std::min<int64_t>(cap32, 9 * max_slots);
                 L->mixed_dinv_off = 4 * L->mixed_val_cap + col_bytes;
                 L->mixed_halo_off = L->mixed_dinv_off + 2304 * (int64_t)sl_max;
-                L->mixed_smem_bytes = (size_t)(L->mixed_halo_off + z_bytes);
+                L->mixed_stage_off = L->mixed_halo_off + z_bytes;
+                L->mixed_smem_bytes = (size_t)(L->mixed_stage_off + stage_bytes);
             }
             if (L->resident || L->mixed_ok) {
                 CK(dupload(m, st, &L->lcol, lcol));
@@ -366,6 +370,7 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
     P.smem_val_cap = mixed ? L->mixed_val_cap : L->smem_val_cap;
     P.smem_dinv_off = L->mixed_dinv_off;
     P.smem_halo_off = L->mixed_halo_off;
+    P.smem_stage_off = L->mixed_stage_off;
     P.lcol = L->lcol;
     P.halo_ptr = L->halo_ptr;
     P.halo_rows = L->halo_rows;

@@ -48,6 +48,7 @@ struct DevLayout {
     bool mixed_ok = false;          /* the mixed solver's shared-memory layout fits */
     int64_t mixed_val_cap = 0;     /* floats staged per CTA */
     int64_t mixed_dinv_off = 0, mixed_halo_off = 0;
+    int64_t mixed_stage_off = 0;     /* halo u, v staging (cp.async) */
     size_t mixed_smem_bytes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;   /* brackets the solver launch */
     int max_grid_alloc() const { return partial_capacity; }

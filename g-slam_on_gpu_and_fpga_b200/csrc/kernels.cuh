@@ -79,6 +79,7 @@ struct PcgParams {
     int64_t smem_val_cap;  /* resident solver: values (multiple of 288) staged in shared memory */
     int64_t smem_dinv_off; /* mixed solver: byte offsets of own-row D^-1 and of z (own + halo rows) */
     int64_t smem_halo_off;
+    int64_t smem_stage_off; /* mixed solver: halo rows' u, v (32 B per row), copied in with cp.async */
     const int *lcol;       /* resident solver: per slot, CTA-local column index (own rows, then halo) */
     const int *halo_ptr;   /* resident solver: [grid + 1] halo list bounds per CTA */
     const int *halo_rows;  /* resident solver: halo rows (new row indices) */

@@ -127,6 +127,39 @@ __device__ __forceinline__ bool grid_reduce_arrive(const double (&v)[NV], double
     return *s_ok != 0;
 }
 
+/* the partial loads of grid_reduce_sum alone (warps < NV), so a caller can issue them
+ * ahead of its own loads and finish with grid_reduce_sum_finish */
+template <int NV>
+__device__ __forceinline__ void grid_reduce_sum_issue(const double *partials_base, int epoch,
+                                                      double (&t)[GSLAM_SUM_UNROLL]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp >= NV) return;
+    const int G = (int)gridDim.x;
+    const double *pp = partials_base + ((epoch - 1) & 1) * 4 * G + warp * G;
+#pragma unroll
+    for (int u = 0; u < GSLAM_SUM_UNROLL; u++) {
+        const int c = lane + 32 * u;
+        t[u] = c < G ? __ldcg(pp + c) : 0.0;
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ void grid_reduce_sum_finish(const double *partials_base, int epoch,
+                                                       const double (&t)[GSLAM_SUM_UNROLL], double *s_bc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp >= NV) return;
+    const int G = (int)gridDim.x;
+    const double *pp = partials_base + ((epoch - 1) & 1) * 4 * G + warp * G;
+    double s = t[0];
+#pragma unroll
+    for (int u = 1; u < GSLAM_SUM_UNROLL; u++) s = s + t[u];
+    for (int c = lane + 32 * GSLAM_SUM_UNROLL; c < G; c += 32) s = s + __ldcg(pp + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) s_bc[warp] = s;
+    if (NV > 1) asm volatile("bar.sync 1, %0;" ::"r"(NV * 32) : "memory");
+}
+
 template <int NV>
 __device__ __forceinline__ void grid_reduce_sum(const double *partials_base, int epoch, double *s_bc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

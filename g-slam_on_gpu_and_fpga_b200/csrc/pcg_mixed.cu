@@ -64,6 +64,16 @@ __device__ __forceinline__ F3 ldf3(const float *v4, int row) {
     return F3{ v.x, v.y, v.z };
 }
 
+/* 16-byte asynchronous global -> shared copy through L2 (no registers), and its wait */
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit_wait_later() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ void stf3(float *v4, int row, F3 v) {
     *reinterpret_cast<float4 *>(v4 + 4 * (size_t)row) = make_float4(v.a, v.b, v.c, 0.f);
 }
@@ -123,6 +133,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     int *scol = reinterpret_cast<int *>(smem + 4 * P.smem_val_cap);
     double *sdinv = reinterpret_cast<double *>(smem + P.smem_dinv_off);
     float *sz = reinterpret_cast<float *>(smem + P.smem_halo_off);
+    float *sstage = reinterpret_cast<float *>(smem + P.smem_stage_off); /* halo u, v: 2 float4 per row */
 
     if (threadIdx.x == 0) {
         tma_mbar_init(&s_bar, 1);
@@ -211,16 +222,24 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
             stf3(PUB_V(1), row, zero);
         }
         if (!grid_barrier(P.gs, (unsigned)(++epoch), P.spin_limit, &s_ok)) { timed_out = true; break; }
-        F3 hz = zero, hu = zero, hv = zero;
-        if (has_h) { hz = ldcgf3(PUB_Z(1), hrow); hu = ldcgf3(PUB_U(1), hrow); hv = ldcgf3(PUB_V(1), hrow); }
+        /* the halo's published (z, u, v) go straight into shared memory (no registers held
+         * across the reduction): z into the halo row's z slot, u and v into staging */
+        if (has_h) {
+            cp_async16(sz + 4 * (n_loc + threadIdx.x), PUB_Z(1) + 4 * (size_t)hrow);
+            cp_async16(sstage + 8 * threadIdx.x, PUB_U(1) + 4 * (size_t)hrow);
+            cp_async16(sstage + 8 * threadIdx.x + 4, PUB_V(1) + 4 * (size_t)hrow);
+            cp_async_commit_wait_later();
+        }
         float alpha = 0.f, beta = 0.f;
         int k = 0;
         while (true) {
             const int pr = (k - 1) & 1, pw = k & 1;
             /* z_k of the halo rows (first: frees the prefetched registers) */
             if (has_h) {
+                cp_async_wait_all();
                 F3 zn, vn;
-                step_zv(hz, hu, hv, alpha, beta, zn, vn);
+                step_zv(ldf3(sz, n_loc + threadIdx.x), ldf3(sstage, 2 * threadIdx.x), ldf3(sstage, 2 * threadIdx.x + 1),
+                        alpha, beta, zn, vn);
                 stf3(sz, n_loc + (int)threadIdx.x, zn);
             }
             if (h_extra) {
@@ -293,8 +312,14 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
                 timed_out = true;
                 break;
             }
-            /* the halo's values for iteration k + 1, in flight while the partials are summed */
-            if (has_h) { hz = ldcgf3(PUB_Z(pw), hrow); hu = ldcgf3(PUB_U(pw), hrow); hv = ldcgf3(PUB_V(pw), hrow); }
+            /* the halo's values for iteration k + 1, in flight while the partials are summed
+             * (every read of the halo z slots in this iteration's SpMV precedes the barrier) */
+            if (has_h) {
+                cp_async16(sz + 4 * (n_loc + threadIdx.x), PUB_Z(pw) + 4 * (size_t)hrow);
+                cp_async16(sstage + 8 * threadIdx.x, PUB_U(pw) + 4 * (size_t)hrow);
+                cp_async16(sstage + 8 * threadIdx.x + 4, PUB_V(pw) + 4 * (size_t)hrow);
+                cp_async_commit_wait_later();
+            }
             grid_reduce_sum<3>(P.partials, epoch, s_bc);
             total++;
             k++;

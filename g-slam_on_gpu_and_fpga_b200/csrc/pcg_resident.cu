@@ -199,9 +199,14 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
             reason = GSLAM_STOP_TIMEOUT;
             break;
         }
-        /* the halo's z_{k+1} and p_k, in flight while the partials are summed */
-        if (has_h) { hz = ldcg3(P.z4, hrow); hp = ldcg3(pnew, hrow); }
-        grid_reduce_sum<2>(P.partials, epoch, s_bc);
+        /* the partials' loads first, then the halo's z_{k+1} and p_k, in flight while
+         * the partials are summed */
+        {
+            double tp[GSLAM_SUM_UNROLL];
+            grid_reduce_sum_issue<2>(P.partials, epoch, tp);
+            if (has_h) { hz = ldcg3(P.z4, hrow); hp = ldcg3(pnew, hrow); }
+            grid_reduce_sum_finish<2>(P.partials, epoch, tp, s_bc);
+        }
         k++;
         if (threadIdx.x == 0) {
             const double rr = s_bc[0], rz_new = s_bc[1];
