@@ -325,30 +325,26 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
             k++;
             if (threadIdx.x == 0) {
                 /* alpha_k = gamma / (delta - beta_k gamma / alpha_{k-1}) = gamma g / (delta g - gamma^2)
-                 * with g = gamma_{k-1} alpha_{k-1}: the products in FP64 (the cancellation
-                 * happens there), the two quotients in FP32 (they are used as FP32 and
-                 * are the recurrence's state: alpha_{k-1} is the value the vectors used) */
+                 * with g = gamma_{k-1} alpha_{k-1}: one FP64 division on the critical path (beta's
+                 * runs beside it); both rounded to FP32 for the vector updates */
                 const double gamma = s_bc[0], delta = s_bc[1], rho = s_bc[2];
                 if (k == 1) s_sc[2] = rho;
-                double num, den;
-                float bt;
-                if (k == 1) { bt = 0.f; num = gamma; den = delta; }
+                double a, bt;
+                if (k == 1) { bt = 0.0; a = gamma / delta; }
                 else {
                     const double g = s_sc[0] * s_sc[1];
-                    bt = (float)gamma / (float)s_sc[0];
-                    num = gamma * g;
-                    den = delta * g - gamma * gamma;
+                    bt = gamma / s_sc[0];
+                    a = (gamma * g) / (delta * g - gamma * gamma);
                 }
-                const float a = (float)num / (float)den;
                 int flag = 0;
-                if (!(delta != 0.0) || !(den != 0.0) || !(a == a) || isinf(a)) flag = 2;
+                if (!(delta != 0.0) || !(a == a) || isinf(a)) flag = 2;
                 else if (rho <= P.inner_tol * P.inner_tol * s_sc[2] || k >= P.inner_max_iter ||
                          total >= P.max_iter || rho < s_sc[3])
                     flag = 1;
                 s_sc[0] = gamma;
-                s_sc[1] = (double)a;
-                s_ab[0] = a;
-                s_ab[1] = bt;
+                s_sc[1] = a;
+                s_ab[0] = (float)a;
+                s_ab[1] = (float)bt;
                 s_flag = flag;
             }
             __syncthreads();
