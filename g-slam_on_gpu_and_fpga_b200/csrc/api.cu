@@ -569,6 +569,7 @@ int gslam_destroy(gslam_graph *g) {
     if (g->batch) {
         if (g->batch->h_res) cudaFreeHost(g->batch->h_res);
         if (g->batch->h_gdiff) cudaFreeHost(g->batch->h_gdiff);
+        if (g->batch->h_gres) cudaFreeHost(g->batch->h_gres);
         delete g->batch;
     }
     if (g->ev_round0) cudaEventDestroy(g->ev_round0);
@@ -1088,14 +1089,13 @@ int gslam_create_se2_batch(const gslam_se2_graph *graphs, uint32_t n_graphs, con
     return GSLAM_OK;
 }
 
+static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total);
+
 static int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total) {
+    if (g->o.precision == GSLAM_PREC_MIXED) return batch_solve_mixed(g, per_graph, total);
     BatchState &B = *g->batch;
     DevLayout *L = &g->L;
     cudaStream_t st = g->st;
-    if (g->o.precision != GSLAM_PREC_FP64) {
-        g_last_error = "the batched solver runs in FP64";
-        return GSLAM_ERR_BAD_INPUT;
-    }
     launch_diag_inv(st, L->n_rows, L->diag_slot, L->val, L->dinv);
     CK(cudaGetLastError());
     PcgParams P;
@@ -1139,7 +1139,7 @@ static int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve
     CK(cudaMemsetAsync(B.d_res, 0, B.n_graphs * sizeof(PcgResult), st));
     CK(cudaMemcpyAsync(B.d_active, &B.n_graphs, sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(L->ev0, st));
-    CK(launch_pcg_batch(st, P, BP, B.grid, B.block, B.smem_bytes));
+    CK(launch_pcg_batch(st, P, BP, B.grid, B.block, B.smem_bytes, false));
     CK(cudaEventRecord(L->ev1, st));
     CK(cudaMemcpyAsync(g->h_res, L->res, sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(B.h_res, B.d_res, B.n_graphs * sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
@@ -1168,6 +1168,158 @@ static int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve
         g_last_error = "solver barrier wait timed out";
         return GSLAM_ERR_DEVICE_TIMEOUT;
     }
+    return GSLAM_OK;
+}
+
+/*
+ * Mixed-precision batch: iterative refinement driven from the host, every graph at
+ * once. Per step: the FP32 right-hand side (the FP64 residual, 0 for graphs already
+ * done), one launch of the batched PCG in FP32 (FP32 values and vectors, FP64 D^-1 and
+ * dot products, per-graph scalars, inner tolerance inner_tol), x += d in FP64, and the
+ * FP64 residual b - A x with per-graph norms. A graph stops at tol, at max_iter inner
+ * iterations, or when a step does not halve its residual; if any graph stagnates the
+ * batch is solved again in FP64 and those results are reported.
+ */
+static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total) {
+    BatchState &B = *g->batch;
+    DevLayout *L = &g->L;
+    cudaStream_t st = g->st;
+    DevMem &m = g->mem;
+    const int G = B.n_graphs;
+    int rc = gslam_layout_ensure_fp32(L, st);
+    if (rc != GSLAM_OK) return rc;
+    if (!L->val32_fresh) {
+        launch_val_to_f32(st, 9 * L->n_slots, L->val, L->val32);
+        L->val32_fresh = true;
+    }
+    if (!B.d_bf4) {
+        CK(dalloc(m, &B.d_bf4, 4 * 32 * (size_t)L->n_slices));
+        CK(dalloc(m, &B.d_gactive, (size_t)G));
+        CK(dalloc(m, &B.d_gres, (size_t)G));
+        CK(cudaMallocHost(&B.h_gres, G * sizeof(double)));
+    }
+    launch_diag_inv(st, L->n_rows, L->diag_slot, L->val, L->dinv);
+    /* x = 0; r = b - A 0 = b with per-graph ||b|| */
+    CK(cudaMemsetAsync(L->x4, 0, 4 * 32 * (size_t)L->n_slices * sizeof(double), st));
+    CK(cudaMemsetAsync(L->q4, 0, 4 * 32 * (size_t)L->n_slices * sizeof(double), st));
+    launch_batch_resid(st, G, B.d_pose_off, L->b4, L->q4, L->r4, B.d_gres);
+    CK(cudaMemcpyAsync(B.h_gres, B.d_gres, G * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<double> bnorm(G), rel(G, 1.0);
+    std::vector<int> its(G, 0), refs(G, 0), reason(G, GSLAM_STOP_MAXIT), active(G, 1);
+    bool stagnated = false;
+    for (int q = 0; q < G; q++) {
+        bnorm[q] = std::sqrt(B.h_gres[q]);
+        if (bnorm[q] == 0.0) { active[q] = 0; reason[q] = GSLAM_STOP_TOL; rel[q] = 0.0; }
+    }
+    PcgParams P;
+    memset(&P, 0, sizeof P);
+    P.n_rows = L->n_rows;
+    P.n_slices = L->n_slices;
+    P.slice_ptr = L->slice_ptr;
+    P.row_len = L->row_len;
+    P.col = L->col;
+    P.val32 = L->val32;
+    P.dinv = L->dinv;
+    P.xf4 = L->f[0]; P.rf4 = L->f[1]; P.zf4 = L->f[2]; P.pfa4 = L->f[3]; P.pfb4 = L->f[4]; P.qf4 = L->f[5];
+    P.tol_rel = g->o.inner_tol;
+    P.gs = L->gs;
+    P.res = L->res;
+    const double ms_lim = g->o.barrier_timeout_ms > 0 ? g->o.barrier_timeout_ms : 2000.0;
+    P.spin_limit = (long long)(ms_lim * (double)L->clock_khz);
+    P.absent_cta = g->o.test_absent_cta;
+    BatchParams BP;
+    memset(&BP, 0, sizeof BP);
+    BP.n_graphs = G;
+    BP.cta_slice = B.d_cta_slice;
+    BP.slice_graph = B.d_slice_graph;
+    BP.cta_g0 = B.d_cta_g0;
+    BP.cta_g1 = B.d_cta_g1;
+    BP.graph_cta0 = B.d_graph_cta0;
+    BP.graph_ncta = B.d_graph_ncta;
+    BP.part_off = B.d_part_off;
+    BP.total_parts = B.total_parts;
+    BP.partials = B.d_partials;
+    BP.res = B.d_res;
+    BP.active = B.d_active;
+    BP.bf4 = B.d_bf4;
+    CK(cudaEventRecord(L->ev0, st));
+    for (int step = 0; step < std::max(g->o.max_refine, 1); step++) {
+        int n_active = 0, used = 0;
+        for (int q = 0; q < G; q++)
+            if (active[q]) { n_active++; used = std::max(used, its[q]); }
+        if (n_active == 0) break;
+        const int cap = std::min(g->o.inner_max_iter, g->o.max_iter - used);
+        if (cap <= 0) break;
+        P.max_iter = cap;
+        CK(cudaMemcpyAsync(B.d_gactive, active.data(), G * sizeof(int), cudaMemcpyHostToDevice, st));
+        launch_batch_rhs32(st, L->n_rows, B.d_slice_graph, B.d_gactive, L->r4, B.d_bf4);
+        CK(cudaMemsetAsync(L->gs, 0, sizeof(GridSync), st));
+        CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
+        CK(cudaMemsetAsync(B.d_res, 0, G * sizeof(PcgResult), st));
+        CK(cudaMemcpyAsync(B.d_active, &G, sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(launch_pcg_batch(st, P, BP, B.grid, B.block, B.smem_bytes, true));
+        launch_batch_add_x(st, L->n_rows, L->f[0], L->x4);
+        launch_spmv64(st, L->n_rows, L->n_slices, L->slice_ptr, L->row_len, L->col, L->val, L->x4, L->q4);
+        launch_batch_resid(st, G, B.d_pose_off, L->b4, L->q4, L->r4, B.d_gres);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(g->h_res, L->res, sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(B.h_res, B.d_res, G * sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(B.h_gres, B.d_gres, G * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (g->h_res->timeout) {
+            g_last_error = "solver barrier wait timed out";
+            return GSLAM_ERR_DEVICE_TIMEOUT;
+        }
+        for (int q = 0; q < G; q++) {
+            if (!active[q]) continue;
+            its[q] += B.h_res[q].iterations;
+            refs[q]++;
+            const double prev = rel[q];
+            rel[q] = std::sqrt(B.h_gres[q]) / bnorm[q];
+            if (rel[q] < g->o.tol) { active[q] = 0; reason[q] = GSLAM_STOP_TOL; }
+            else if (its[q] >= g->o.max_iter || refs[q] >= g->o.max_refine) { active[q] = 0; reason[q] = GSLAM_STOP_MAXIT; }
+            else if (rel[q] > 0.5 * prev) { active[q] = 0; reason[q] = GSLAM_STOP_STAGNATION; stagnated = true; }
+        }
+    }
+    CK(cudaEventRecord(L->ev1, st));
+    CK(cudaEventSynchronize(L->ev1));
+    float solve_ms = 0.f;
+    cudaEventElapsedTime(&solve_ms, L->ev0, L->ev1);
+    if (stagnated) {
+        /* the FP32 inner solves cannot resolve at least one graph: FP64 for the batch */
+        gslam_solve_stats s64;
+        gslam_opts keep = g->o;
+        g->o.precision = GSLAM_PREC_FP64;
+        rc = batch_solve(g, per_graph, &s64);
+        g->o = keep;
+        if (per_graph)
+            for (int q = 0; q < G; q++) {
+                per_graph[q].iterations += its[q];
+                per_graph[q].refinements = -refs[q];
+                per_graph[q].solve_ms += solve_ms;
+            }
+        if (total) { *total = s64; total->solve_ms += solve_ms; }
+        return rc;
+    }
+    gslam_solve_stats agg;
+    memset(&agg, 0, sizeof agg);
+    agg.solve_ms = solve_ms;
+    for (int q = 0; q < G; q++) {
+        if (per_graph) {
+            memset(&per_graph[q], 0, sizeof per_graph[q]);
+            per_graph[q].iterations = its[q];
+            per_graph[q].refinements = refs[q];
+            per_graph[q].reason = reason[q];
+            per_graph[q].rel_residual = rel[q];
+            per_graph[q].solve_ms = solve_ms;
+        }
+        agg.iterations = std::max(agg.iterations, its[q]);
+        agg.refinements = std::max(agg.refinements, refs[q]);
+        agg.rel_residual = std::max(agg.rel_residual, rel[q]);
+        if (reason[q] != GSLAM_STOP_TOL) agg.reason = reason[q];
+    }
+    if (total) *total = agg;
     return GSLAM_OK;
 }
 

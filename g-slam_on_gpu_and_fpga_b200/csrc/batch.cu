@@ -36,8 +36,92 @@
 
 #define BATCH_LG_MAX 32 /* graphs one CTA may touch */
 
-template <int BS>
+/* ---- row-vector access for either precision of the inner solve ----
+ * T = double: the reference's FP64 PCG; T = float: the inner solve of the mixed
+ * batch (FP32 values and vectors, FP64 D^-1 and dot products). Rows are padded to
+ * 4 elements. */
+template <typename T> struct TV { T a, b, c; };
+
+__device__ __forceinline__ TV<double> tv_ld(const double *v4, int row) { const V3 v = ld3(v4, row); return { v.a, v.b, v.c }; }
+__device__ __forceinline__ TV<double> tv_ldg(const double *v4, int row) { const V3 v = ldg3(v4, row); return { v.a, v.b, v.c }; }
+__device__ __forceinline__ TV<double> tv_ldcg(const double *v4, int row) { const V3 v = ldcg3(v4, row); return { v.a, v.b, v.c }; }
+__device__ __forceinline__ void tv_st(double *v4, int row, TV<double> v) { st3(v4, row, V3{ v.a, v.b, v.c }); }
+__device__ __forceinline__ TV<float> tv_ld(const float *v4, int row) {
+    const float4 v = *reinterpret_cast<const float4 *>(v4 + 4 * (size_t)row);
+    return { v.x, v.y, v.z };
+}
+__device__ __forceinline__ TV<float> tv_ldg(const float *v4, int row) {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(v4 + 4 * (size_t)row));
+    return { v.x, v.y, v.z };
+}
+__device__ __forceinline__ TV<float> tv_ldcg(const float *v4, int row) {
+    const float4 v = __ldcg(reinterpret_cast<const float4 *>(v4 + 4 * (size_t)row));
+    return { v.x, v.y, v.z };
+}
+__device__ __forceinline__ void tv_st(float *v4, int row, TV<float> v) {
+    *reinterpret_cast<float4 *>(v4 + 4 * (size_t)row) = make_float4(v.a, v.b, v.c, 0.f);
+}
+
+/* p = z + beta p_old (first iteration: p = z), as MatrixOps.c:382, for a neighbour row */
+template <typename T>
+__device__ __forceinline__ TV<T> tv_p_of(const T *z4, const T *pold4, int row, T beta, bool first) {
+    const TV<T> z = tv_ldcg(z4, row);
+    if (first) return z;
+    const TV<T> p = tv_ldcg(pold4, row);
+    return { z.a + beta * p.a, z.b + beta * p.b, z.c + beta * p.c };
+}
+
+/* z = D^-1 r with the FP64 block, rounded to T */
+template <typename T>
+__device__ __forceinline__ TV<T> tv_dinv(const double *dinv, int row, TV<T> r) {
+    const V3 z = apply_dinv(dinv, row, V3{ (double)r.a, (double)r.b, (double)r.c });
+    return { (T)z.a, (T)z.b, (T)z.c };
+}
+
+/* q = A p for one row, blocks in ascending column order (spmv_row for either type) */
+template <typename T>
+__device__ __forceinline__ TV<T> tv_spmv_row(const T *vb, const int *cb, int len, const T *z4, const T *pold,
+                                              T beta, bool first) {
+    T q0 = 0, q1 = 0, q2 = 0;
+    int j = 0;
+    for (; j + 1 < len; j += 2) {
+        const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
+        const TV<T> p0 = tv_p_of(z4, pold, c0, beta, first), p1 = tv_p_of(z4, pold, c1, beta, first);
+        const T *v0 = vb + 288 * j, *v1 = v0 + 288;
+        q0 = q0 + __ldg(v0) * p0.a;       q0 = q0 + __ldg(v0 + 32) * p0.b;  q0 = q0 + __ldg(v0 + 64) * p0.c;
+        q1 = q1 + __ldg(v0 + 96) * p0.a;  q1 = q1 + __ldg(v0 + 128) * p0.b; q1 = q1 + __ldg(v0 + 160) * p0.c;
+        q2 = q2 + __ldg(v0 + 192) * p0.a; q2 = q2 + __ldg(v0 + 224) * p0.b; q2 = q2 + __ldg(v0 + 256) * p0.c;
+        q0 = q0 + __ldg(v1) * p1.a;       q0 = q0 + __ldg(v1 + 32) * p1.b;  q0 = q0 + __ldg(v1 + 64) * p1.c;
+        q1 = q1 + __ldg(v1 + 96) * p1.a;  q1 = q1 + __ldg(v1 + 128) * p1.b; q1 = q1 + __ldg(v1 + 160) * p1.c;
+        q2 = q2 + __ldg(v1 + 192) * p1.a; q2 = q2 + __ldg(v1 + 224) * p1.b; q2 = q2 + __ldg(v1 + 256) * p1.c;
+    }
+    if (j < len) {
+        const int c0 = __ldg(cb + 32 * j);
+        const TV<T> p0 = tv_p_of(z4, pold, c0, beta, first);
+        const T *v0 = vb + 288 * j;
+        q0 = q0 + __ldg(v0) * p0.a;       q0 = q0 + __ldg(v0 + 32) * p0.b;  q0 = q0 + __ldg(v0 + 64) * p0.c;
+        q1 = q1 + __ldg(v0 + 96) * p0.a;  q1 = q1 + __ldg(v0 + 128) * p0.b; q1 = q1 + __ldg(v0 + 160) * p0.c;
+        q2 = q2 + __ldg(v0 + 192) * p0.a; q2 = q2 + __ldg(v0 + 224) * p0.b; q2 = q2 + __ldg(v0 + 256) * p0.c;
+    }
+    return { q0, q1, q2 };
+}
+
+/* the solve's vectors for either precision */
+template <typename T> struct BVec;
+template <> struct BVec<double> {
+    const double *val, *b; double *x, *r, *z, *pa, *pb, *q;
+    __device__ BVec(const PcgParams &P, const BatchParams &) : val(P.val), b(P.b4), x(P.x4), r(P.r4), z(P.z4),
+        pa(P.p4a), pb(P.p4b), q(P.q4) {}
+};
+template <> struct BVec<float> {
+    const float *val, *b; float *x, *r, *z, *pa, *pb, *q;
+    __device__ BVec(const PcgParams &P, const BatchParams &B) : val(P.val32), b(B.bf4), x(P.xf4), r(P.rf4),
+        z(P.zf4), pa(P.pfa4), pb(P.pfb4), q(P.qf4) {}
+};
+
+template <int BS, typename T>
 __global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B) {
+    const BVec<T> V(P, B);
     extern __shared__ __align__(16) double s_part[]; /* [slices of this CTA][2] */
     __shared__ double s_rz[BATCH_LG_MAX], s_rr[BATCH_LG_MAX], s_bn[BATCH_LG_MAX];
     __shared__ double s_alpha[BATCH_LG_MAX], s_beta[BATCH_LG_MAX];
@@ -103,13 +187,14 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B)
         const int row = 32 * (s0 + sl) + lane;
         double rz = 0.0, rr = 0.0;
         if (row < P.n_rows) {
-            const V3 b = ldg3(P.b4, row);
-            st3(P.x4, row, V3{ 0.0, 0.0, 0.0 });
-            st3(P.r4, row, b);
-            const V3 z = apply_dinv(P.dinv, row, b);
-            st3(P.z4, row, z);
-            rz = rz + b.a * z.a; rz = rz + b.b * z.b; rz = rz + b.c * z.c;
-            rr = rr + b.a * b.a; rr = rr + b.b * b.b; rr = rr + b.c * b.c;
+            const TV<T> b = tv_ldg(V.b, row);
+            tv_st(V.x, row, TV<T>{ 0, 0, 0 });
+            tv_st(V.r, row, b);
+            const TV<T> z = tv_dinv(P.dinv, row, b);
+            tv_st(V.z, row, z);
+            const double b0 = b.a, b1 = b.b, b2 = b.c;
+            rz = rz + b0 * (double)z.a; rz = rz + b1 * (double)z.b; rz = rz + b2 * (double)z.c;
+            rr = rr + b0 * b0; rr = rr + b1 * b1; rr = rr + b2 * b2;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -136,8 +221,8 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B)
     while (!timed_out) {
         if (k >= P.max_iter) break;
         const bool first = (k == 0);
-        double *pnew = (k & 1) ? P.p4b : P.p4a;
-        const double *pold = (k & 1) ? P.p4a : P.p4b;
+        T *pnew = (k & 1) ? V.pb : V.pa;
+        const T *pold = (k & 1) ? V.pa : V.pb;
         /* ---- phase A: p = z + beta p, q = A p, per-graph p.q ---- */
         for (int sl = warp; sl < ns; sl += W) {
             const int s = s0 + sl;
@@ -145,14 +230,15 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B)
             const int row = 32 * s + lane;
             double pq = 0.0;
             if (!s_done[t] && row < P.n_rows) {
-                const double beta = s_beta[t];
-                const V3 pn = p_of(P.z4, pold, row, beta, first);
-                st3(pnew, row, pn);
+                const T beta = (T)s_beta[t];
+                const TV<T> pn = tv_p_of(V.z, pold, row, beta, first);
+                tv_st(pnew, row, pn);
                 const int64_t sb = __ldg(P.slice_ptr + s);
-                const V3 q = spmv_row(P.val + 9 * sb + lane, P.col + sb + lane, __ldg(P.row_len + row), P.z4,
-                                      pold, beta, first);
-                st3(P.q4, row, q);
-                pq = pq + pn.a * q.a; pq = pq + pn.b * q.b; pq = pq + pn.c * q.c;
+                const TV<T> q = tv_spmv_row(V.val + 9 * sb + lane, P.col + sb + lane, __ldg(P.row_len + row), V.z,
+                                            pold, beta, first);
+                tv_st(V.q, row, q);
+                pq = pq + (double)pn.a * (double)q.a; pq = pq + (double)pn.b * (double)q.b;
+                pq = pq + (double)pn.c * (double)q.c;
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) pq = pq + __shfl_down_sync(0xffffffffu, pq, o);
@@ -184,17 +270,18 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B)
             const int row = 32 * s + lane;
             double rr = 0.0, rz = 0.0;
             if (!s_done[t] && row < P.n_rows) {
-                const double alpha = s_alpha[t];
-                const V3 pn = ld3(pnew, row), q = ld3(P.q4, row);
-                V3 x = ld3(P.x4, row), r = ld3(P.r4, row);
+                const T alpha = (T)s_alpha[t];
+                const TV<T> pn = tv_ld(pnew, row), q = tv_ld(V.q, row);
+                TV<T> x = tv_ld(V.x, row), r = tv_ld(V.r, row);
                 x.a = x.a + alpha * pn.a; x.b = x.b + alpha * pn.b; x.c = x.c + alpha * pn.c;
                 r.a = r.a - alpha * q.a;  r.b = r.b - alpha * q.b;  r.c = r.c - alpha * q.c;
-                st3(P.x4, row, x);
-                st3(P.r4, row, r);
-                rr = rr + r.a * r.a; rr = rr + r.b * r.b; rr = rr + r.c * r.c;
-                const V3 z = apply_dinv(P.dinv, row, r);
-                st3(P.z4, row, z);
-                rz = rz + r.a * z.a; rz = rz + r.b * z.b; rz = rz + r.c * z.c;
+                tv_st(V.x, row, x);
+                tv_st(V.r, row, r);
+                const double r0 = r.a, r1 = r.b, r2 = r.c;
+                rr = rr + r0 * r0; rr = rr + r1 * r1; rr = rr + r2 * r2;
+                const TV<T> z = tv_dinv(P.dinv, row, r);
+                tv_st(V.z, row, z);
+                rz = rz + r0 * (double)z.a; rz = rz + r1 * (double)z.b; rz = rz + r2 * (double)z.c;
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -241,21 +328,19 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B)
     }
 }
 
-template <int BS>
-static const void *batch_fn() { return (const void *)k_pcg_batch<BS>; }
-
+template <typename T>
 static const void *batch_kernel(int block) {
     switch (block) {
-    case 256: return batch_fn<256>();
-    case 512: return batch_fn<512>();
-    case 1024: return batch_fn<1024>();
+    case 256: return (const void *)k_pcg_batch<256, T>;
+    case 512: return (const void *)k_pcg_batch<512, T>;
+    case 1024: return (const void *)k_pcg_batch<1024, T>;
     default: return nullptr;
     }
 }
 
 cudaError_t launch_pcg_batch(cudaStream_t st, const PcgParams &p, const BatchParams &b, int grid, int block,
-                             size_t smem_bytes) {
-    const void *fn = batch_kernel(block);
+                             size_t smem_bytes, bool fp32) {
+    const void *fn = fp32 ? batch_kernel<float>(block) : batch_kernel<double>(block);
     if (!fn) return cudaErrorInvalidValue;
     PcgParams pc = p;
     BatchParams bc = b;
@@ -264,12 +349,13 @@ cudaError_t launch_pcg_batch(cudaStream_t st, const PcgParams &p, const BatchPar
 }
 
 int pcg_batch_max_grid(int block, size_t smem_bytes, int device) {
-    const void *fn = batch_kernel(block);
-    if (!fn) return 0;
-    int n_sm = 0, per = 0;
+    const void *f64 = batch_kernel<double>(block), *f32 = batch_kernel<float>(block);
+    if (!f64 || !f32) return 0;
+    int n_sm = 0, a = 0, b = 0;
     if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, smem_bytes) != cudaSuccess) return 0;
-    return per * n_sm;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, f64, block, smem_bytes) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f32, block, smem_bytes) != cudaSuccess) return 0;
+    return std::min(a, b) * n_sm;
 }
 
 int pcg_batch_lg_max() { return BATCH_LG_MAX; }
@@ -317,4 +403,66 @@ void launch_add_diag(cudaStream_t st, int n, const int64_t *slots, const double 
 void launch_batch_diff(cudaStream_t st, int n_graphs, const int *pose_off, const int *n_real, const double *dx,
                        double *out) {
     if (n_graphs > 0) k_batch_diff<<<n_graphs, 256, 0, st>>>(pose_off, n_real, dx, out);
+}
+
+/* ---- the mixed batch's refinement steps (FP64) ---- */
+
+/* rhs of the FP32 inner solve: bf4 = (float) r4 for rows of active graphs, else 0 */
+__global__ void k_batch_rhs32(int n_rows, const int *__restrict__ slice_graph, const int *__restrict__ active,
+                              const double *__restrict__ r4, float *__restrict__ bf4) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n_rows) return;
+    const bool on = active[slice_graph[row >> 5]] != 0;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (on) v = make_float4((float)r4[4 * (size_t)row], (float)r4[4 * (size_t)row + 1], (float)r4[4 * (size_t)row + 2], 0.f);
+    reinterpret_cast<float4 *>(bf4)[row] = v;
+}
+
+/* x4 += xf4 (the FP32 correction, accumulated in FP64) */
+__global__ void k_batch_add_x(int n_rows, const float *__restrict__ xf4, double *__restrict__ x4) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n_rows) return;
+    const float4 d = reinterpret_cast<const float4 *>(xf4)[row];
+    double *x = x4 + 4 * (size_t)row;
+    x[0] = x[0] + (double)d.x;
+    x[1] = x[1] + (double)d.y;
+    x[2] = x[2] + (double)d.z;
+}
+
+/* r4 = b4 - q4 (q4 = A x) and each graph's ||r||^2, one CTA per graph */
+__global__ void k_batch_resid(const int *__restrict__ pose_off, const double *__restrict__ b4,
+                              const double *__restrict__ q4, double *__restrict__ r4, double *__restrict__ out) {
+    __shared__ double sh[32];
+    const int g = blockIdx.x;
+    const int r0 = pose_off[g], r1 = pose_off[g + 1];
+    double acc = 0.0;
+    for (int i = 3 * r0 + threadIdx.x; i < 3 * r1; i += blockDim.x) {
+        const int row = i / 3, c = i - 3 * row;
+        const double r = b4[4 * (size_t)row + c] - q4[4 * (size_t)row + c];
+        r4[4 * (size_t)row + c] = r;
+        acc = acc + r * r;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc = acc + __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = s + sh[w];
+        out[g] = s;
+    }
+}
+
+void launch_batch_rhs32(cudaStream_t st, int n_rows, const int *slice_graph, const int *active, const double *r4,
+                        float *bf4) {
+    k_batch_rhs32<<<(n_rows + 255) / 256, 256, 0, st>>>(n_rows, slice_graph, active, r4, bf4);
+}
+
+void launch_batch_add_x(cudaStream_t st, int n_rows, const float *xf4, double *x4) {
+    k_batch_add_x<<<(n_rows + 255) / 256, 256, 0, st>>>(n_rows, xf4, x4);
+}
+
+void launch_batch_resid(cudaStream_t st, int n_graphs, const int *pose_off, const double *b4, const double *q4,
+                        double *r4, double *out) {
+    k_batch_resid<<<n_graphs, 256, 0, st>>>(pose_off, b4, q4, r4, out);
 }

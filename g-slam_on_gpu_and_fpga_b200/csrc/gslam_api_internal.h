@@ -73,6 +73,10 @@ struct BatchState {
     PcgResult *d_res = nullptr, *h_res = nullptr;
     double *h_gdiff = nullptr;
     int *d_active = nullptr;
+    /* mixed batches: FP32 right-hand side, per-graph active flags and residual norms */
+    float *d_bf4 = nullptr;
+    int *d_gactive = nullptr;
+    double *d_gres = nullptr, *h_gres = nullptr;
 };
 
 struct gslam_graph {

@@ -107,12 +107,20 @@ struct BatchParams {
     double *partials;        /* [2 buffers][2 values][total_parts] */
     PcgResult *res;          /* [n_graphs] */
     int *active;             /* graphs still iterating (set to n_graphs before launch) */
+    const float *bf4;        /* FP32 inner solve: right-hand side (padded rows) */
 };
+/* fp32: the inner solve of the mixed batch (FP32 values / vectors in PcgParams' FP32
+ * fields, right-hand side bf4); otherwise the FP64 PCG on val / b4. */
 cudaError_t launch_pcg_batch(cudaStream_t st, const PcgParams &p, const BatchParams &b, int grid, int block,
-                             size_t smem_bytes);
+                             size_t smem_bytes, bool fp32);
 int pcg_batch_max_grid(int block, size_t smem_bytes, int device);
 int pcg_batch_lg_max();
 void launch_add_diag(cudaStream_t st, int n, const int64_t *slots, const double *anchor, double *val);
+void launch_batch_rhs32(cudaStream_t st, int n_rows, const int *slice_graph, const int *active, const double *r4,
+                        float *bf4);
+void launch_batch_add_x(cudaStream_t st, int n_rows, const float *xf4, double *x4);
+void launch_batch_resid(cudaStream_t st, int n_graphs, const int *pose_off, const double *b4, const double *q4,
+                        double *r4, double *out);
 void launch_batch_diff(cudaStream_t st, int n_graphs, const int *pose_off, const int *n_real, const double *dx,
                        double *out);
 

@@ -76,3 +76,36 @@ def test_lambda_sweep_in_one_batch(pkg, graphs):
         assert stats[q].reason == 0
         assert np.linalg.norm(b.graph_poses(q, poses) - ref) <= 1e-4 * np.linalg.norm(ref - cg.init)
     b.close()
+
+
+def test_mixed_batch_truncated_matches_fp64_residuals(pkg, graphs):
+    """The reference's per-round settings (tol 1e-6, 500 iterations): the mixed batch
+    (FP32 inner PCG, FP64 refinement) ends every graph at the FP64 batch's residual."""
+    res = {}
+    for prec in (0, 1):
+        b = pkg.PoseGraphBatch.from_se2_list(graphs, LAMS, angle_wrap=1, precision=prec)
+        res[prec] = b.round_all()
+        b.close()
+    for q in range(len(graphs)):
+        f, m = res[0][q], res[1][q]
+        if f.reason == 0:
+            assert m.reason == 0
+        else:
+            assert m.iterations == f.iterations == 500
+            assert m.rel_residual <= 1.5 * f.rel_residual + 1e-9, (q, m.rel_residual, f.rel_residual)
+
+
+def test_mixed_batch_converged_matches_fp64(pkg, graphs):
+    """Converged solves: every graph reaches the FP64 tolerance (refinement, or FP64 after
+    a stagnating graph) and the poses agree with the FP64 batch."""
+    opts = dict(tol=1e-8, max_iter=20000, angle_wrap=1, max_refine=200)
+    poses = {}
+    for prec in (0, 1):
+        b = pkg.PoseGraphBatch.from_se2_list(graphs, LAMS, precision=prec, **opts)
+        st = b.round_all()
+        assert all(s.reason == 0 and s.rel_residual < 1e-8 for s in st), [(s.reason, s.rel_residual) for s in st]
+        poses[prec] = [b.graph_poses(q).copy() for q in range(len(graphs))]
+        b.close()
+    for q, cg in enumerate(graphs):
+        d = np.linalg.norm(poses[1][q] - poses[0][q]) / np.linalg.norm(poses[0][q] - cg.init)
+        assert d <= 1e-5, (q, d)
