@@ -39,7 +39,7 @@ EXPORTS = [
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
     "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_set_se2_weights", "gslam_adjoint",
     "gslam_create_se2_batch", "gslam_batch_round", "gslam_batch_layout",
-    "gslam_gj_inverse", "gslam_gj_solve",
+    "gslam_gj_inverse", "gslam_gj_solve", "gslam_landmark_map",
 ]
 
 
@@ -164,6 +164,7 @@ def lib() -> C.CDLL:
             "gslam_batch_layout": [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
             "gslam_gj_inverse": [C.c_int, VP, C.c_int, VP, C.POINTER(C.c_float)],
             "gslam_gj_solve": [C.c_int, VP, C.c_int, VP, VP, VP, C.POINTER(C.c_float)],
+            "gslam_landmark_map": [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), DP],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

@@ -509,6 +509,17 @@ int gslam_create_reference(const gslam_reference_graph *in, const gslam_opts *op
                     cudaMemcpyHostToDevice, g->st);
     std::vector<unsigned> zs(in->obs_step, in->obs_step + in->n_obs);
     std::vector<double> zrb(in->obs, in->obs + 2 * (size_t)in->n_obs);
+    {
+        std::vector<int64_t> lptr;
+        std::vector<unsigned> lmem;
+        gslam_landmark_groups(in->n_obs, in->obs_landmark, &g->lm_ids, &lptr, &lmem);
+        if (dupload(m, g->st, &g->d_lm_ptr, lptr) != cudaSuccess ||
+            dupload(m, g->st, &g->d_lm_members, lmem) != cudaSuccess ||
+            dalloc(m, &g->d_lm_ms, 2 * std::max<size_t>(g->lm_ids.size(), 1)) != cudaSuccess) {
+            g_last_error = "upload failed";
+            return fail(GSLAM_ERR_CUDA);
+        }
+    }
     if (dupload(m, g->st, &g->d_z_step, zs) != cudaSuccess ||
         dupload(m, g->st, &g->d_z_rb, zrb) != cudaSuccess ||
         dupload(m, g->st, &g->d_pj, pj) != cudaSuccess ||
@@ -1359,5 +1370,22 @@ int gslam_batch_layout(gslam_graph *g, uint32_t *n_graphs, uint32_t *pose_offset
     *n_graphs = (uint32_t)g->batch->n_graphs;
     if (pose_offset)
         for (int q = 0; q <= g->batch->n_graphs; q++) pose_offset[q] = (uint32_t)g->batch->pose_off[q];
+    return GSLAM_OK;
+}
+
+int gslam_landmark_map(gslam_graph *g, uint32_t *n_landmarks, uint32_t *ids, double *ms) {
+    if (!g || !n_landmarks) BAD("null argument");
+    if (g->factors != GSLAM_FACTORS_REFERENCE) BAD("the landmark map belongs to reference-factor graphs");
+    const int n = (int)g->lm_ids.size();
+    *n_landmarks = (uint32_t)n;
+    if (!ids && !ms) return GSLAM_OK;
+    if (ids)
+        for (int i = 0; i < n; i++) ids[i] = g->lm_ids[i];
+    if (ms) {
+        launch_landmark_map(g->st, n, g->d_lm_ptr, g->d_lm_members, g->d_z_step, g->d_z_rb, g->d_poses, g->d_lm_ms);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(ms, g->d_lm_ms, 2 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, g->st));
+        CK(cudaStreamSynchronize(g->st));
+    }
     return GSLAM_OK;
 }

@@ -105,6 +105,11 @@ struct gslam_graph {
     double *d_csr_tmp = nullptr, *d_xi_tmp = nullptr;
     double *d_adj = nullptr;   /* adjoint: rhs, mu (3 N each), per-edge gradient (3 E) */
     BatchState *batch = nullptr; /* non-null for a batch of graphs */
+    /* landmark groups of the z list (reference graphs) */
+    std::vector<unsigned> lm_ids;
+    int64_t *d_lm_ptr = nullptr;
+    unsigned *d_lm_members = nullptr;
+    double *d_lm_ms = nullptr;
     PcgResult *h_res = nullptr;
     double *h_diff = nullptr;
     PcgResult last_res = {};

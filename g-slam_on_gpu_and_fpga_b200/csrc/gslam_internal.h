@@ -68,6 +68,10 @@ int gslam_build_structure_ex(int n_rows, int64_t n_edges, const unsigned *t1, co
                              int sell_window, const std::vector<int> *diag_rows,
                              const std::vector<int> *segments, gslam_structure *s);
 
+/* Landmark groups of the z list (first-appearance order, members in z order). */
+void gslam_landmark_groups(int64_t n_z, const unsigned *z_lm, std::vector<unsigned> *ids,
+                           std::vector<int64_t> *ptr, std::vector<unsigned> *members);
+
 /* Reference edge order for observation edges (GSLAM.c:222-318): pairs of z-list indices. */
 void gslam_obs_pairs(int64_t n_z, const unsigned *z_lm, std::vector<unsigned> *pj,
                      std::vector<unsigned> *pk);

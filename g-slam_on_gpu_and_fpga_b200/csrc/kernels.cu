@@ -375,3 +375,34 @@ void launch_pose_update(cudaStream_t st, int n_rows, const int *iperm, const dou
     k_pose_update<<<n_blocks, 256, 0, st>>>(n_rows, iperm, x4, poses, dx, wrap, block_sums);
     k_finish_diff<<<1, 32, 0, st>>>(n_blocks, block_sums, 3.0 * n_rows, diff_out);
 }
+
+/* ------------------------------------------------------------------------ */
+/* landmark map (GSLAM.c:141-196, MapEdge.c:7-32, vec_mean MatrixOps.c:161-171) */
+/* ------------------------------------------------------------------------ */
+
+/* one thread per landmark: mean over its observations (z order, sums from 0.0) of
+ * (x + r cos(theta + phi), y + r sin(theta + phi)) at the observing pose */
+__global__ void k_landmark_map(int n_groups, const int64_t *__restrict__ ptr, const unsigned *__restrict__ members,
+                               const unsigned *__restrict__ z_step, const double *__restrict__ z_rb,
+                               const double *__restrict__ poses, double *__restrict__ ms) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_groups) return;
+    double m0 = 0.0, m1 = 0.0;
+    const int64_t a = ptr[g], b = ptr[g + 1];
+    for (int64_t q = a; q < b; q++) {
+        const unsigned z = members[q];
+        const double *x = poses + 3 * (size_t)z_step[z];
+        double s, c;
+        cr_sincos(x[2] + z_rb[2 * (size_t)z + 1], &s, &c);
+        m0 = m0 + (x[0] + z_rb[2 * (size_t)z] * c);
+        m1 = m1 + (x[1] + z_rb[2 * (size_t)z] * s);
+    }
+    ms[2 * g] = m0 / (double)(b - a);
+    ms[2 * g + 1] = m1 / (double)(b - a);
+}
+
+void launch_landmark_map(cudaStream_t st, int n_groups, const int64_t *ptr, const unsigned *members,
+                         const unsigned *z_step, const double *z_rb, const double *poses, double *ms) {
+    if (n_groups > 0)
+        k_landmark_map<<<blocks_for(n_groups, 128), 128, 0, st>>>(n_groups, ptr, members, z_step, z_rb, poses, ms);
+}

@@ -86,6 +86,9 @@ struct PcgParams {
     int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
 };
 
+void launch_landmark_map(cudaStream_t st, int n_groups, const int64_t *ptr, const unsigned *members,
+                         const unsigned *z_step, const double *z_rb, const double *poses, double *ms);
+
 /* SpMV of n_copies matrices sharing one block pattern, in one launch (pcg.cu). */
 void launch_spmv_multi64(cudaStream_t st, int n_copies, int n_rows, int n_slices, const int64_t *slice_ptr,
                          const int *row_len, const int *col, const double *val, int64_t stride,

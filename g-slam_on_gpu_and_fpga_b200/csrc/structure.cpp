@@ -251,6 +251,37 @@ int gslam_build_structure_ex(int n_rows, int64_t n_edges, const unsigned *t1, co
     return GSLAM_OK;
 }
 
+/* Landmarks in order of first appearance in the z list, each with its z indices in
+ * z-list order: the grouping of make_edges' landmark_keys_zlist (GSLAM.c:246-261). */
+void gslam_landmark_groups(int64_t n_z, const unsigned *z_lm, std::vector<unsigned> *ids,
+                           std::vector<int64_t> *ptr, std::vector<unsigned> *members) {
+    ids->clear();
+    ptr->assign(1, 0);
+    members->clear();
+    std::vector<std::pair<unsigned, int64_t>> byid(n_z);
+    for (int64_t i = 0; i < n_z; i++) byid[i] = {z_lm[i], i};
+    std::stable_sort(byid.begin(), byid.end(),
+                     [](const std::pair<unsigned, int64_t> &a, const std::pair<unsigned, int64_t> &b) {
+                         return a.first < b.first;
+                     });
+    struct group { int64_t begin, end; };
+    std::vector<group> groups;
+    for (int64_t i = 0; i < n_z;) {
+        int64_t j = i;
+        while (j < n_z && byid[j].first == byid[i].first) j++;
+        groups.push_back({i, j});
+        i = j;
+    }
+    std::sort(groups.begin(), groups.end(), [&](const group &a, const group &b) {
+        return byid[a.begin].second < byid[b.begin].second;
+    });
+    for (const group &gr : groups) {
+        ids->push_back(byid[gr.begin].first);
+        for (int64_t a = gr.begin; a < gr.end; a++) members->push_back((unsigned)byid[a].second);
+        ptr->push_back((int64_t)members->size());
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* host-only C ABI utilities                                                 */
 /* ------------------------------------------------------------------------ */

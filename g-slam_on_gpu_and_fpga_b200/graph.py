@@ -234,6 +234,15 @@ class PoseGraph:
         abi.check(abi.lib().gslam_get_dx(self._h, abi.ptr(out)))
         return out
 
+    def landmark_map(self):
+        """(landmark ids, positions [L, 2]) at the current poses (reference-factor graphs)."""
+        n = C.c_uint32()
+        abi.check(abi.lib().gslam_landmark_map(self._h, C.byref(n), None, None))
+        ids = np.zeros(n.value, np.uint32)
+        ms = np.zeros((max(n.value, 1), 2))
+        abi.check(abi.lib().gslam_landmark_map(self._h, C.byref(n), abi.ptr(ids, C.c_uint32), abi.ptr(ms)))
+        return ids, ms[:n.value]
+
     # ---- differentiation (SE(2) graphs) ----
     def set_weights(self, lam: float, log_w=None) -> None:
         """New lambda and (optionally) per-edge log information weights [E, 3]."""

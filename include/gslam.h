@@ -227,6 +227,16 @@ int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *d_col_idx,
                            int max_iter, void *stream, gslam_solve_stats *stats);
 
 /*
+ * Landmark map of a reference-factor graph at its current poses (GSLAM.c:141-196 with
+ * MapEdge_create, MapEdge.c:7-32): for every landmark, in order of first appearance in
+ * the observation list, the mean over its observations of
+ * (x + r cos(theta + phi), y + r sin(theta + phi)). *n_landmarks receives the count;
+ * ids (n entries) and ms (2 per landmark, host) may be NULL to query the count only.
+ * (The reference computes this map and frees it; here it is returned.)
+ */
+int gslam_landmark_map(gslam_graph *g, uint32_t *n_landmarks, uint32_t *ids, double *ms);
+
+/*
  * Batches of independent SE(2) graphs (no counterpart in the reference, which solves
  * one graph per process and sweeps lambda with a shell loop).
  *

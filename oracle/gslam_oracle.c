@@ -475,6 +475,13 @@ int or_run(int use_cr, unsigned n_poses, double *poses, const double *u_nu_om, d
 /* dense Gauss-Jordan inverse (MatrixOps.c:29-91), heap workspace             */
 /* ------------------------------------------------------------------------ */
 
+int or_landmark_map(int use_cr, unsigned n_groups, const long *group_ptr, const unsigned *members,
+                    const unsigned *z_step, const double *z_rb, const double *poses, double *ms) {
+    if (use_cr) landmark_map_cr(n_groups, group_ptr, members, z_step, z_rb, poses, ms);
+    else landmark_map_glibc(n_groups, group_ptr, members, z_step, z_rb, poses, ms);
+    return 0;
+}
+
 int or_gj_inverse(unsigned n, const double *a, double *res) {
     double *t = malloc(sizeof(double) * (size_t)n * n);
     if (!t) return -1;

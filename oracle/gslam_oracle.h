@@ -53,6 +53,8 @@ int or_run(int use_cr, unsigned n_poses, double *poses, const double *u_nu_om, d
            int *pcg_iters);
 
 int or_gj_inverse(unsigned n, const double *a, double *res);
+int or_landmark_map(int use_cr, unsigned n_groups, const long *group_ptr, const unsigned *members,
+                    const unsigned *z_step, const double *z_rb, const double *poses, double *ms);
 
 int or_csr_build_anchor(unsigned dim, long n_edges, const unsigned *t1, const unsigned *t2,
                         const double *blocks, double anchor, int *row_ptr, int *col_idx,

@@ -243,6 +243,33 @@ def cr_sincos(x: float):
     return s.value, c.value
 
 
+def landmark_groups(z_lm):
+    """Landmarks in order of first appearance in the z list, each with its z indices in
+    z-list order (the order of make_edges' landmark_keys_zlist, GSLAM.c:246-261)."""
+    z_lm = np.asarray(z_lm)
+    first = {}
+    for i, lm in enumerate(z_lm.tolist()):
+        first.setdefault(lm, []).append(i)
+    ids = list(first)                      # dict keeps first-appearance order
+    ptr = np.zeros(len(ids) + 1, np.int64)
+    members = []
+    for k, lm in enumerate(ids):
+        members += first[lm]
+        ptr[k + 1] = len(members)
+    return np.array(ids, np.uint32), ptr, np.array(members, np.uint32)
+
+
+def landmark_map(g: Graph, poses, cr: bool = True):
+    """(landmark ids, positions [L, 2]) after a run, as GSLAM.c:141-196 computes them."""
+    L = lib()
+    ids, ptr, members = landmark_groups(g.z_lm)
+    poses = np.ascontiguousarray(poses, np.float64)
+    ms = np.zeros((max(len(ids), 1), 2))
+    L.or_landmark_map(int(cr), len(ids), _p(ptr, C.c_long), _p(members, C.c_uint), _p(g.z_step, C.c_uint),
+                      _p(g.z_rb, C.c_double), _p(poses, C.c_double), _p(ms, C.c_double))
+    return ids, ms[:len(ids)]
+
+
 def gj_inverse(a):
     L = lib()
     a = np.ascontiguousarray(a, np.float64)
@@ -288,6 +315,10 @@ class _LKZ(C.Structure):
     _fields_ = [("landmark_id", C.c_uint), ("z", _Z)]
 
 
+class _MapEdge(C.Structure):
+    _fields_ = [("x", _HX), ("z", _Z), ("m", C.c_double * 2), ("Omega", C.c_double * 4), ("xi", C.c_double * 2)]
+
+
 class _CSR(C.Structure):
     _fields_ = [("row_ptr", C.POINTER(C.c_int)), ("col_idx", C.POINTER(C.c_int)),
                 ("values", C.POINTER(C.c_double)), ("dim", C.c_int), ("nnz", C.c_int)]
@@ -314,6 +345,9 @@ def ref():
         R.pcg_solve_sparse.argtypes = [C.POINTER(C.c_double), C.POINTER(_CSR),
                                        C.POINTER(C.c_double), C.c_uint]
         R.free_csr.argtypes = [C.POINTER(_CSR)]
+        R.MapEdge_create.argtypes = [C.POINTER(_MapEdge), _Z, _Z, C.POINTER(_HX), C.POINTER(C.c_double)]
+        R.MapEdge_create.restype = C.POINTER(_MapEdge)
+        R.vec_mean.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_uint, C.c_uint]
         _ref = R
     return _ref
 
@@ -370,6 +404,38 @@ def ref_round(g: Graph, poses, lam: float):
     R.pcg_solve_sparse(_p(dx, C.c_double), C.byref(csr), _p(xi, C.c_double), dim)
     R.free_csr(C.byref(csr))
     return t1, t2, blocks, (row_ptr, col_idx, values), xi, dx
+
+
+def ref_landmark_map(g: Graph, poses):
+    """The landmark map as the reference program builds it after its last round
+    (GSLAM.c:141-196): make_edges' landmark-sorted z list, one MapEdge_create per
+    observation and vec_mean per landmark, all the reference's own compiled functions.
+    Landmark ids equal to the z count (the reference's loop sentinel) are not supported."""
+    R = ref()
+    hx, _, zs = _ref_arrays(g, poses)
+    n_z = len(g.z_lm)
+    pj, _ = obs_pairs(g.z_lm)
+    edges = (_Edge * max(len(pj), 1))()
+    lkz = (_LKZ * max(n_z, 1))()
+    ne = C.c_uint(0); nl = C.c_uint(0)
+    R.make_edges(hx, g.n_poses, zs, n_z, edges, C.byref(ne), lkz, C.byref(nl))
+    snr = (C.c_double * 2)(0.14, 0.05)
+    ids, ms = [], []
+    group = []
+    for i in range(nl.value):
+        if i == 0 or lkz[i].landmark_id != lkz[i - 1].landmark_id:
+            ids.append(lkz[i].landmark_id)
+            head = lkz[i].z
+            group = []
+        me = _MapEdge()
+        R.MapEdge_create(C.byref(me), lkz[i].z, head, hx, snr)
+        group.append((me.m[0], me.m[1]))
+        if i == nl.value - 1 or lkz[i].landmark_id != lkz[i + 1].landmark_id:
+            m = np.ascontiguousarray(group, np.float64)
+            mean = np.zeros(2)
+            R.vec_mean(_p(mean, C.c_double), _p(m, C.c_double), 2, len(group))
+            ms.append(mean)
+    return np.array(ids, np.uint32), np.array(ms, np.float64).reshape(-1, 2)
 
 
 def ref_run_binary(log_path: str, lam: float, rounds: int, dump_path: str, use_diff: int = 1):

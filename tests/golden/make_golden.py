@@ -5,7 +5,8 @@
 Each fixture holds the inputs of a reference-format log produced by the
 package's city-grid generator and the C oracle's outputs for it: edge blocks in
 both math flavours (glibc and correctly rounded), the reference CSR, xi, one
-PCG solution at the reference's settings, and the poses after a short run. The
+PCG solution at the reference's settings, the poses after a short run and the
+landmark map at those poses. The
 oracle itself is pinned bit for bit against the reference build in
 tests/test_oracle_pin.py; these fixtures carry that pin to machines without the
 reference tree.
@@ -44,6 +45,7 @@ def make(case):
     out["row_ptr"], out["col_idx"], out["values"], out["xi"] = O.csr_build(g.dim, t1, t2, b)
     out["dx"], _, _ = O.pcg(out["row_ptr"], out["col_idx"], out["values"], out["xi"])
     out["poses_run"], _, _ = O.run(g, lam, case["rounds"], cr=False)
+    out["lm_ids"], out["lm_ms"] = O.landmark_map(g, out["poses_run"], cr=False)
     np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **out)
 
 

@@ -259,6 +259,31 @@ def test_bad_observation_step_rejected():
     assert e.value.code == G.abi.ERR_BAD_INPUT
 
 
+def test_landmark_map_bitwise(oracle):
+    """The device landmark map (GSLAM.c:141-196) after two rounds, bit for bit against
+    the oracle's correctly rounded flavour at the same poses."""
+    G = load_pkg()
+    for seed, n in ((7, 600), (8, 2500)):
+        log = G.synth.landmark_log(n, seed=seed)
+        og = _ograph(oracle, log)
+        with G.PoseGraph.from_log(log, 0.1) as g:
+            for _ in range(2):
+                g.round()
+            ids, ms = g.landmark_map()
+            poses = g.poses
+        ids_o, ms_o = oracle.landmark_map(og, poses, cr=True)
+        assert len(ids) > 1 and np.array_equal(ids, ids_o)
+        assert_bitwise(ms, ms_o, f"landmarks{n} map")
+
+
+def test_landmark_map_rejected_for_se2(oracle):
+    G = load_pkg()
+    cg = G.synth.city_grid(64, seed=3, block=8)
+    with G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w) as g:
+        with pytest.raises(G.abi.GslamError):
+            g.landmark_map()
+
+
 def test_single_pose_and_two_poses(oracle):
     G = load_pkg()
     for n in (1, 2):

@@ -80,6 +80,33 @@ def test_reference_defect_above_21845_documented(oracle):
     assert ci.max() == dim - 1
 
 
+@pytest.mark.parametrize("name,lam", [("cityTrees100.log.txt", 0.1), ("cityTrees1k.log.txt", 1.0),
+                                      ("victoria-park-100.log.txt", 0.06)])
+def test_landmark_map_bitwise_vs_reference(oracle, name, lam):
+    """The post-run landmark map (GSLAM.c:141-196) against the reference's own
+    make_edges, MapEdge_create and vec_mean, at the logged poses and after two rounds;
+    the correctly rounded flavour stays within a few ulps of it."""
+    _need_ref(oracle)
+    g = oracle.read_log(ref_data(name))
+    p, _, _ = oracle.run(g, lam, 2, cr=False)
+    for poses in (g.x, p):
+        ids_r, ms_r = oracle.ref_landmark_map(g, poses)
+        ids, ms = oracle.landmark_map(g, poses, cr=False)
+        assert np.array_equal(ids, ids_r)
+        assert_bitwise(ms, ms_r, f"{name} landmark map")
+        _, ms_cr = oracle.landmark_map(g, poses, cr=True)
+        assert np.abs(ms_cr - ms).max() <= 1e-13 * max(1.0, np.abs(ms).max())
+
+
+def test_landmark_groups_first_appearance():
+    """Landmarks come in order of first appearance; members in z order."""
+    import oracle as O
+    ids, ptr, members = O.landmark_groups([7, 3, 7, 9, 3, 3])
+    assert ids.tolist() == [7, 3, 9]
+    assert ptr.tolist() == [0, 2, 5, 6]
+    assert members.tolist() == [0, 2, 1, 4, 5, 3]
+
+
 @pytest.mark.skipif(not os.environ.get("GSLAM_SLOW"), reason="116 GN rounds at N=7120 (set GSLAM_SLOW=1)")
 def test_victoria_park_golden_dump(oracle):
     """The committed reference dump of `GSLAM 1 1.0 200 1 victoria-park.log.txt`."""
@@ -113,3 +140,6 @@ def test_golden_fixtures(oracle, path):
     assert_bitwise(x, z["dx"], "dx")
     p, _, _ = oracle.run(g, lam, int(z["rounds"]), cr=False)
     assert_bitwise(p, z["poses_run"], "poses after run")
+    ids, ms = oracle.landmark_map(g, p, cr=False)
+    assert np.array_equal(ids, z["lm_ids"])
+    assert_bitwise(ms, z["lm_ms"], "landmark map")
