@@ -13,6 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libgslam.so")
 CLI_PATH = os.path.join(HERE, "bin", "GSLAM")
+DATA_TOOL_PATH = os.path.join(HERE, "bin", "gslam-data")
 
 OK = 0
 ERR_BAD_INPUT = -1
@@ -39,7 +40,7 @@ EXPORTS = [
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
     "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_set_se2_weights", "gslam_adjoint",
     "gslam_create_se2_batch", "gslam_batch_round", "gslam_batch_layout",
-    "gslam_gj_inverse", "gslam_gj_solve", "gslam_landmark_map",
+    "gslam_gj_inverse", "gslam_gj_solve", "gslam_landmark_map", "gslam_cost",
 ]
 
 
@@ -165,6 +166,7 @@ def lib() -> C.CDLL:
             "gslam_gj_inverse": [C.c_int, VP, C.c_int, VP, C.POINTER(C.c_float)],
             "gslam_gj_solve": [C.c_int, VP, C.c_int, VP, VP, VP, C.POINTER(C.c_float)],
             "gslam_landmark_map": [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), DP],
+            "gslam_cost": [VP, DP, DP],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

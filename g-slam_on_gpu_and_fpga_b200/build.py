@@ -2,7 +2,8 @@
 
     python g-slam_on_gpu_and_fpga_b200/build.py [--force]
 
-Outputs: g-slam_on_gpu_and_fpga_b200/lib/libgslam.so, g-slam_on_gpu_and_fpga_b200/bin/GSLAM.
+Outputs: g-slam_on_gpu_and_fpga_b200/lib/libgslam.so, g-slam_on_gpu_and_fpga_b200/bin/GSLAM and
+the host-only dataset tool g-slam_on_gpu_and_fpga_b200/bin/gslam-data (g++).
 nvcc cross-compiles for sm_100a without a GPU. Every translation unit is built
 with -fmad=false: the FP64 path must round every product and sum separately to
 match the reference's arithmetic; FP32 kernels call fused multiply-adds
@@ -23,6 +24,7 @@ INC = os.path.join(ROOT, "include")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "lib", "libgslam.so")
 CLI = os.path.join(PKG, "bin", "GSLAM")
+DATA_TOOL = os.path.join(PKG, "bin", "gslam-data")
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -32,6 +34,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC"
 LIB_SOURCES = ["structure.cpp", "kernels.cu", "pcg.cu", "pcg_resident.cu", "pcg_mixed.cu", "pcg_static.cu",
                "adjoint.cu", "batch.cu", "gj.cu", "api.cu", "dropin.cu", "logio.cpp"]
 CLI_SOURCES = ["cli.cpp"]
+DATA_SOURCES = ["datasets.cpp"]
+# the dataset tool reproduces CPython's float arithmetic: C library math calls kept as calls
+DATA_FLAGS = ["-O2", "-std=c++17", "-ffp-contract=off", "-fno-builtin", "-fno-fast-math"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:
@@ -74,6 +79,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or _newer(CLI, cli_src + [LIB] + headers):
         _run([NVCC, *ARCH, *COMMON, "-o", CLI, *cli_src, "-L", os.path.dirname(LIB), "-lgslam",
               "-Xlinker", "-rpath,$ORIGIN/../lib"])
+    data_src = [os.path.join(CSRC, s) for s in DATA_SOURCES]
+    if force or _newer(DATA_TOOL, data_src):
+        _run([os.environ.get("CXX", "g++"), *DATA_FLAGS, "-o", DATA_TOOL, *data_src, "-lm"])
     if verbose:
         print("built", LIB, "and", CLI)
     return LIB

@@ -1389,3 +1389,25 @@ int gslam_landmark_map(gslam_graph *g, uint32_t *n_landmarks, uint32_t *ids, dou
     }
     return GSLAM_OK;
 }
+
+int gslam_cost(gslam_graph *g, double *cost, double *edge_costs) {
+    if (!g || !cost) BAD("null argument");
+    if (g->factors != GSLAM_FACTORS_REFERENCE) BAD("the round cost belongs to reference-factor graphs");
+    DevMem &m = g->mem;
+    if (!g->d_cost) {
+        CK(dalloc(m, &g->d_edge_cost, std::max<size_t>((size_t)g->n_edges, 1)));
+        CK(dalloc(m, &g->d_cost_blocks, (size_t)edge_cost_blocks(g->n_edges)));
+        CK(dalloc(m, &g->d_cost, 1));
+    }
+    launch_edge_costs(g->st, g->n_obs_edges, g->n_poses, g->d_pj, g->d_pk, g->d_z_step, g->d_z_rb,
+                      g->d_controls, g->delta, g->lambda, g->mns, g->d_poses, g->d_edge_cost,
+                      g->d_cost_blocks, g->d_cost);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(g->h_diff, g->d_cost, sizeof(double), cudaMemcpyDeviceToHost, g->st));
+    if (edge_costs)
+        CK(cudaMemcpyAsync(edge_costs, g->d_edge_cost, (size_t)g->n_edges * sizeof(double),
+                           cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    *cost = *g->h_diff;
+    return GSLAM_OK;
+}

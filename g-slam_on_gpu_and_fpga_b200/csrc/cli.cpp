@@ -5,10 +5,12 @@
  *
  * use_diff = 1: diff = ||dx|| / sqrt(dim), stop below 0.01 or after 20 rounds
  *               without a new best (GSLAM.c:104-130).
- * use_diff = 0: the reference CPU program's cost criterion reads past the end of a
- *               2-element array and never resets its accumulator (GSLAM.c:74-87);
- *               like the reference GPU program (src/gpu_pcg_fp64/GSLAM.cu:165-171)
- *               this falls back to the norm criterion.
+ * use_diff = 0: the cost criterion of GSLAM.c:74-87 and :108-136, diff =
+ *               |cost - last_cost| / cost, stop below 1e-8, with the cost that code
+ *               meant: computed afresh each round at the round's starting poses
+ *               (gslam_cost). The reference CPU program reads a 3-vector out of a
+ *               2-element array and never resets its sum; the reference GPU program
+ *               (src/gpu_pcg_fp64/GSLAM.cu:165-171) uses the norm criterion instead.
  * Options beyond the reference, in the environment (defaults reproduce it):
  *   GSLAM_TOL (1e-6), GSLAM_MAXIT (500), GSLAM_PREC (fp64 | mixed), GSLAM_WRAP (0),
  *   GSLAM_STATS=1 prints one JSON line of solver statistics per round on stderr.
@@ -39,7 +41,6 @@ int main(int argc, char *argv[]) {
     const double lambda = atof(argv[2]);
     const unsigned rounds = (unsigned)atoi(argv[3]);
     const unsigned draw = (unsigned)atoi(argv[4]);
-    (void)use_diff;
 
     gslam_log *log = nullptr;
     if (gslam_read_log(argv[5], &log) != GSLAM_OK) {
@@ -84,25 +85,33 @@ int main(int argc, char *argv[]) {
         fprintf(stderr, "gslam: %s (%d)\n", gslam_last_error(), rc);
         return 1;
     }
-    double best = 1e30;
+    double best = 1e30, last_cost = 0.0;
     unsigned no_improve = 0;
     for (unsigned n = 1; n <= rounds; n++) {
+        double cost = 0.0;
+        if (!use_diff) rc = gslam_cost(g, &cost, nullptr);
         gslam_solve_stats st;
-        rc = gslam_round(g, &st);
+        if (rc == GSLAM_OK) rc = gslam_round(g, &st);
         if (rc != GSLAM_OK) {
             fprintf(stderr, "gslam: %s (%d)\n", gslam_last_error(), rc);
             gslam_destroy(g);
             return 1;
         }
-        printf("%d rounds executed: %.17g\n", n, st.diff);
+        const double diff = use_diff ? st.diff : fabs(cost - last_cost) / cost;
+        printf("%d rounds executed: %.17g\n", n, diff);
         if (stats_json)
             fprintf(stderr,
                     "{\"round\": %u, \"pcg_iterations\": %d, \"refinements\": %d, \"reason\": %d, "
-                    "\"rel_residual\": %.6e, \"diff\": %.17g}\n",
-                    n, st.iterations, st.refinements, st.reason, st.rel_residual, st.diff);
-        if (st.diff < 0.01) break;
-        if (st.diff < best) { best = st.diff; no_improve = 0; }
-        else if (++no_improve >= 20) break;
+                    "\"rel_residual\": %.6e, \"diff\": %.17g, \"update_norm\": %.17g}\n",
+                    n, st.iterations, st.refinements, st.reason, st.rel_residual, diff, st.diff);
+        if (use_diff) {
+            if (diff < 0.01) break;
+            if (diff < best) { best = diff; no_improve = 0; }
+            else if (++no_improve >= 20) break;
+        } else {
+            if (diff < 1e-8) break;
+            last_cost = cost;
+        }
     }
     if (draw >= 1) {
         const char *dump = getenv("POSE_DUMP_FILE");

@@ -81,9 +81,11 @@ EM_FN void em_inv(double *res, const double *m) {
 /*
  * ObsEdge (ObsEdge.c:10-212): poses x1, x2 (x, y, theta), observations z1, z2
  * (range, bearing). out[42] = UL, UR, BL, BR (row-major 3x3), xi_u[3], xi_b[3].
+ * cost_out (may be null) receives hat_e^T Omega hat_e with the 2x2 Omega, times the
+ * edge's lambda of 1.0: the GSLAM.c:74-87 cost term with the dimensions it meant.
  */
 EM_FN void em_obs_edge(const double *x1, const double *x2, const double *z1, const double *z2,
-                       double *out) {
+                       double *out, double *cost_out = nullptr) {
     const double snr0 = 0.14, snr1 = 0.05;
     double s1, c1, s2, c2;
     cr_sincos(x1[2] + z1[1], &s1, &c1);
@@ -106,6 +108,12 @@ EM_FN void em_obs_edge(const double *x1, const double *x2, const double *z1, con
 #pragma unroll
     for (int i = 0; i < 4; i++) Sig[i] = S1[i] + S2[i];
     em_inv<2>(Om, Sig);
+    if (cost_out) {
+        double t[2], c;
+        em_dot<1, 2, 2>(t, e, Om);
+        em_dot<1, 2, 1>(&c, t, e);
+        *cost_out = c * 1.0;
+    }
     double B1[6] = { -1.0, -0.0, z1[0] * s1, -0.0, -1.0, -z1[0] * c1 };
     double B2[6] = { 1.0, 0.0, -z2[0] * s2, 0.0, 1.0, z2[0] * c2 };
     double tB1[6], tB2[6], tB1Om[6], tB2Om[6];
@@ -128,10 +136,13 @@ EM_FN void em_obs_edge(const double *x1, const double *x2, const double *z1, con
 
 /*
  * MotionEdge (MotionEdge.c:9-193) between consecutive poses with the control
- * (nu, omega) of the second step. Same 42-double output.
+ * (nu, omega) of the second step. Same 42-double output. cost_out (may be null)
+ * receives lambda d^T Omega d with d = x2 - state_transition(x1), the motion term of
+ * the cost (the reference stores hat_e = 0 for motion edges, MotionEdge.c:187-190).
  */
 EM_FN void em_motion_edge(const double *x1, const double *x2, double nu, double omega,
-                          double delta, double lambda, const double *mns, double *out) {
+                          double delta, double lambda, const double *mns, double *out,
+                          double *cost_out = nullptr) {
     if (fabs(omega) < 1e-5) omega = 1e-5;
     const double M[4] = { mns[0] * mns[0] * fabs(nu) / delta + mns[1] * mns[1] * fabs(omega) / delta,
                           0.0, 0.0,
@@ -188,6 +199,12 @@ EM_FN void em_motion_edge(const double *x1, const double *x2, double nu, double 
     double d[3], v[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) d[i] = x2[i] - xp[i];
+    if (cost_out) {
+        double t[3], c;
+        em_dot<1, 3, 3>(t, d, Om);
+        em_dot<1, 3, 1>(&c, t, d);
+        *cost_out = c * lambda;
+    }
     em_dot<3, 3, 1>(v, tFOm, d);
 #pragma unroll
     for (int i = 0; i < 3; i++) out[36 + i] = v[i] * lambda;

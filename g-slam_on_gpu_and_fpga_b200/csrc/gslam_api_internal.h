@@ -112,6 +112,8 @@ struct gslam_graph {
     double *d_lm_ms = nullptr;
     PcgResult *h_res = nullptr;
     double *h_diff = nullptr;
+    /* round cost: per-edge terms, block sums, total (allocated on first use) */
+    double *d_edge_cost = nullptr, *d_cost_blocks = nullptr, *d_cost = nullptr;
     PcgResult last_res = {};
     cudaEvent_t ev_round0 = nullptr, ev_round1 = nullptr;
 };

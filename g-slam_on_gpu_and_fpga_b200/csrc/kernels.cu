@@ -295,6 +295,61 @@ __global__ void k_finish_diff(int n_blocks, const double *__restrict__ block_sum
     }
 }
 
+/*
+ * Round cost (GSLAM.c:74-87 with the intended dimensions): one thread per edge in the
+ * reference's array order (observation edges, then motion edges), the edge's term
+ * computed by the linearisation's own arithmetic, stored per edge and summed per block
+ * (warp tree, then warps in order); k_finish_cost adds the block sums in block order.
+ */
+__global__ void k_edge_costs(int64_t n_obs_edges, int n_poses, const unsigned *__restrict__ pair_j,
+                             const unsigned *__restrict__ pair_k, const unsigned *__restrict__ z_step,
+                             const double *__restrict__ z_rb, const double *__restrict__ controls,
+                             double delta, double lambda, double m0, double m1, double m2, double m3,
+                             const double *__restrict__ poses, double *__restrict__ edge_cost,
+                             double *__restrict__ block_sums) {
+    __shared__ double sh[32];
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n_edges = n_obs_edges + (n_poses > 1 ? n_poses - 1 : 0);
+    double c = 0.0, out[42];
+    if (e < n_obs_edges) {
+        const unsigned a = pair_j[e], b = pair_k[e];
+        const unsigned s1 = z_step[a], s2 = z_step[b];
+        double x1[3], x2[3], z1[2], z2[2];
+#pragma unroll
+        for (int i = 0; i < 3; i++) { x1[i] = poses[3 * (size_t)s1 + i]; x2[i] = poses[3 * (size_t)s2 + i]; }
+        z1[0] = z_rb[2 * (size_t)a]; z1[1] = z_rb[2 * (size_t)a + 1];
+        z2[0] = z_rb[2 * (size_t)b]; z2[1] = z_rb[2 * (size_t)b + 1];
+        em_obs_edge(x1, x2, z1, z2, out, &c);
+    } else if (e < n_edges) {
+        const int i = (int)(e - n_obs_edges);
+        const double mns[4] = { m0, m1, m2, m3 };
+        double x1[3], x2[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) { x1[k] = poses[3 * (size_t)i + k]; x2[k] = poses[3 * (size_t)(i + 1) + k]; }
+        const double nu = controls[2 * (size_t)(i + 1)], om = controls[2 * (size_t)(i + 1) + 1];
+        em_motion_edge(x1, x2, nu, om, delta, lambda, mns, out, &c);
+    }
+    if (e < n_edges) edge_cost[e] = c;
+    double acc = c;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc = acc + __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = s + sh[w];
+        block_sums[blockIdx.x] = s;
+    }
+}
+
+__global__ void k_finish_cost(int n_blocks, const double *__restrict__ block_sums, double *__restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < n_blocks; i++) s = s + block_sums[i];
+        *out = s;
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* launch helpers                                                            */
 /* ------------------------------------------------------------------------ */
@@ -405,4 +460,17 @@ void launch_landmark_map(cudaStream_t st, int n_groups, const int64_t *ptr, cons
                          const unsigned *z_step, const double *z_rb, const double *poses, double *ms) {
     if (n_groups > 0)
         k_landmark_map<<<blocks_for(n_groups, 128), 128, 0, st>>>(n_groups, ptr, members, z_step, z_rb, poses, ms);
+}
+
+int edge_cost_blocks(int64_t n_edges) { return (int)blocks_for(n_edges > 0 ? n_edges : 1, 128); }
+
+void launch_edge_costs(cudaStream_t st, int64_t n_obs_edges, int n_poses, const unsigned *pj, const unsigned *pk,
+                       const unsigned *z_step, const double *z_rb, const double *controls, double delta,
+                       double lambda, const double *mns, const double *poses, double *edge_cost,
+                       double *block_sums, double *total) {
+    const int64_t n_edges = n_obs_edges + (n_poses > 1 ? n_poses - 1 : 0);
+    const int nb = edge_cost_blocks(n_edges);
+    k_edge_costs<<<nb, 128, 0, st>>>(n_obs_edges, n_poses, pj, pk, z_step, z_rb, controls, delta, lambda,
+                                     mns[0], mns[1], mns[2], mns[3], poses, edge_cost, block_sums);
+    k_finish_cost<<<1, 32, 0, st>>>(nb, block_sums, total);
 }

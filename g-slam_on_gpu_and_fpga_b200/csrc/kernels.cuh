@@ -86,6 +86,14 @@ struct PcgParams {
     int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
 };
 
+/* Round cost terms per edge and their total (kernels.cu); block_sums holds
+ * edge_cost_blocks(n_edges) doubles. */
+int edge_cost_blocks(int64_t n_edges);
+void launch_edge_costs(cudaStream_t st, int64_t n_obs_edges, int n_poses, const unsigned *pj, const unsigned *pk,
+                       const unsigned *z_step, const double *z_rb, const double *controls, double delta,
+                       double lambda, const double *mns, const double *poses, double *edge_cost,
+                       double *block_sums, double *total);
+
 void launch_landmark_map(cudaStream_t st, int n_groups, const int64_t *ptr, const unsigned *members,
                          const unsigned *z_step, const double *z_rb, const double *poses, double *ms);
 

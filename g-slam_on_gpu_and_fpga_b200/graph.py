@@ -234,6 +234,15 @@ class PoseGraph:
         abi.check(abi.lib().gslam_get_dx(self._h, abi.ptr(out)))
         return out
 
+    def cost(self, per_edge: bool = False):
+        """Round cost at the current poses (reference-factor graphs); with per_edge,
+        (total, terms in the reference's edge order)."""
+        tot = C.c_double()
+        n = self.sizes()["n_edges"] if per_edge else 0
+        terms = np.zeros(max(n, 1)) if per_edge else None
+        abi.check(abi.lib().gslam_cost(self._h, C.byref(tot), abi.ptr(terms) if per_edge else None))
+        return (tot.value, terms[:n]) if per_edge else tot.value
+
     def landmark_map(self):
         """(landmark ids, positions [L, 2]) at the current poses (reference-factor graphs)."""
         n = C.c_uint32()

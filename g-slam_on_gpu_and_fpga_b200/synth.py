@@ -17,10 +17,13 @@ Two outputs for one walk:
 """
 from __future__ import annotations
 
+import os
+import subprocess
 from dataclasses import dataclass
 
 import numpy as np
 
+from . import abi
 from .graph import ReferenceLog
 
 
@@ -189,6 +192,27 @@ def write_log(path: str, log: ReferenceLog) -> None:
             f.write(f"x {int(log.x_step[s])} {r(log.x[s, 0])} {r(log.x[s, 1])} {r(log.x[s, 2])}\n")
             for k in zs_by_step.get(s, []):
                 f.write(f"z {int(log.z_step[k])} {int(log.z_lm[k])} {r(log.z[k, 0])} {r(log.z[k, 1])}\n")
+
+
+def _data_tool(*args) -> str:
+    if not os.path.exists(abi.DATA_TOOL_PATH):
+        raise FileNotFoundError(f"{abi.DATA_TOOL_PATH} is not built (python g-slam_on_gpu_and_fpga_b200/build.py)")
+    r = subprocess.run([abi.DATA_TOOL_PATH, *map(str, args)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr.strip() or f"gslam-data failed ({r.returncode})")
+    return r.stdout
+
+
+def generate_citytrees(n_poses: int, path: str, seed: int = 42) -> str:
+    """The reference's cityTrees generator (data/generate_citytrees.py) through the
+    native gslam-data tool: the same file, byte for byte, for the same arguments.
+    Returns the tool's summary lines."""
+    return _data_tool("citytrees", int(n_poses), path, int(seed))
+
+
+def convert_slampp(input_path: str, path: str, delta: float = 1.0) -> str:
+    """The reference's SLAM++ converter (data/convert_slampp.py) through gslam-data."""
+    return _data_tool("slampp", input_path, path, repr(float(delta)))
 
 
 def landmark_log(n: int, seed: int = 0, density: float = 3.0e-3, strip: float = 20.0,

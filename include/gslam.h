@@ -227,6 +227,18 @@ int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *d_col_idx,
                            int max_iter, void *stream, gslam_solve_stats *stats);
 
 /*
+ * Round cost of a reference-factor graph at its current poses: the cost that the
+ * reference's use_diff = 0 criterion accumulates (GSLAM.c:74-87), with the dimensions
+ * that code meant: sum over edges, in the reference's edge order, of
+ * hat_e^T Omega hat_e (observation edges: 2-vector, 2x2 Omega, lambda 1.0) and
+ * lambda d^T Omega d (motion edges, d = x2 - state_transition(x1)). The reference reads
+ * a 3-vector out of its 2-element hat_e and never resets the sum between rounds; this
+ * is computed afresh at each call. edge_costs (host, n_edges entries, may be NULL)
+ * receives the per-edge terms.
+ */
+int gslam_cost(gslam_graph *g, double *cost, double *edge_costs);
+
+/*
  * Landmark map of a reference-factor graph at its current poses (GSLAM.c:141-196 with
  * MapEdge_create, MapEdge.c:7-32): for every landmark, in order of first appearance in
  * the observation list, the mean over its observations of

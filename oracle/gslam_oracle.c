@@ -177,10 +177,10 @@ int or_linearise(int use_cr, unsigned n_poses, const double *poses, const double
         t1[e] = s1; t2[e] = s2;
         if (use_cr)
             or_obs_edge_cr(poses + 3 * (size_t)s1, poses + 3 * (size_t)s2, z_rb + 2 * (size_t)a,
-                           z_rb + 2 * (size_t)b, blocks + 42 * (size_t)e, NULL);
+                           z_rb + 2 * (size_t)b, blocks + 42 * (size_t)e, NULL, NULL);
         else
             or_obs_edge_glibc(poses + 3 * (size_t)s1, poses + 3 * (size_t)s2, z_rb + 2 * (size_t)a,
-                              z_rb + 2 * (size_t)b, blocks + 42 * (size_t)e, NULL);
+                              z_rb + 2 * (size_t)b, blocks + 42 * (size_t)e, NULL, NULL);
     }
     for (unsigned i = 0; i + 1 < n_poses; i++) {
         long e = n_obs_edges + i;
@@ -188,11 +188,50 @@ int or_linearise(int use_cr, unsigned n_poses, const double *poses, const double
         double nu = u_nu_om[2 * (size_t)(i + 1)], om = u_nu_om[2 * (size_t)(i + 1) + 1];
         if (use_cr)
             or_motion_edge_cr(poses + 3 * (size_t)i, poses + 3 * (size_t)(i + 1), nu, om, delta,
-                              lambda, mns, blocks + 42 * (size_t)e);
+                              lambda, mns, blocks + 42 * (size_t)e, NULL);
         else
             or_motion_edge_glibc(poses + 3 * (size_t)i, poses + 3 * (size_t)(i + 1), nu, om, delta,
-                                 lambda, mns, blocks + 42 * (size_t)e);
+                                 lambda, mns, blocks + 42 * (size_t)e, NULL);
     }
+    return 0;
+}
+
+/*
+ * Round cost at `poses` (GSLAM.c:74-87, with the dimensions that code meant and reset
+ * every round): per edge in the reference's array order, observation edges
+ * hat_e^T Omega hat_e (2x2) and motion edges lambda d^T Omega d (3x3); the total is
+ * `cost += c` from 0.0 in that order. edge_cost (may be NULL) receives the terms.
+ */
+int or_round_cost(int use_cr, unsigned n_poses, const double *poses, const double *u_nu_om,
+                  double delta, double lambda, const double *mns, const unsigned *z_step,
+                  const double *z_rb, long n_obs_edges, const unsigned *pj, const unsigned *pk,
+                  double *edge_cost, double *total) {
+    double out[42], acc = 0.0, c;
+    for (long e = 0; e < n_obs_edges; e++) {
+        unsigned a = pj[e], b = pk[e];
+        unsigned s1 = z_step[a], s2 = z_step[b];
+        if (s1 >= n_poses || s2 >= n_poses) return -1;
+        if (use_cr)
+            or_obs_edge_cr(poses + 3 * (size_t)s1, poses + 3 * (size_t)s2, z_rb + 2 * (size_t)a,
+                           z_rb + 2 * (size_t)b, out, NULL, &c);
+        else
+            or_obs_edge_glibc(poses + 3 * (size_t)s1, poses + 3 * (size_t)s2, z_rb + 2 * (size_t)a,
+                              z_rb + 2 * (size_t)b, out, NULL, &c);
+        if (edge_cost) edge_cost[e] = c;
+        acc += c;
+    }
+    for (unsigned i = 0; i + 1 < n_poses; i++) {
+        double nu = u_nu_om[2 * (size_t)(i + 1)], om = u_nu_om[2 * (size_t)(i + 1) + 1];
+        if (use_cr)
+            or_motion_edge_cr(poses + 3 * (size_t)i, poses + 3 * (size_t)(i + 1), nu, om, delta,
+                              lambda, mns, out, &c);
+        else
+            or_motion_edge_glibc(poses + 3 * (size_t)i, poses + 3 * (size_t)(i + 1), nu, om, delta,
+                                 lambda, mns, out, &c);
+        if (edge_cost) edge_cost[n_obs_edges + i] = c;
+        acc += c;
+    }
+    *total = acc;
     return 0;
 }
 

@@ -19,13 +19,15 @@ int or_read_log(const char *path, double *delta,
 long or_obs_edge_pairs(unsigned n_z, const unsigned *z_lm, unsigned *pj, unsigned *pk, long cap);
 
 void or_obs_edge_glibc(const double *x1, const double *x2, const double *z1, const double *z2,
-                       double *out, double *hat_e_out);
+                       double *out, double *hat_e_out, double *cost_out);
 void or_obs_edge_cr(const double *x1, const double *x2, const double *z1, const double *z2,
-                    double *out, double *hat_e_out);
+                    double *out, double *hat_e_out, double *cost_out);
 void or_motion_edge_glibc(const double *x1, const double *x2, double nu, double omega,
-                          double delta, double lambda, const double *mns, double *out);
+                          double delta, double lambda, const double *mns, double *out,
+                          double *cost_out);
 void or_motion_edge_cr(const double *x1, const double *x2, double nu, double omega,
-                       double delta, double lambda, const double *mns, double *out);
+                       double delta, double lambda, const double *mns, double *out,
+                       double *cost_out);
 double or_norm_glibc(const double *v, unsigned n);
 double or_norm_cr(const double *v, unsigned n);
 
@@ -34,6 +36,11 @@ int or_linearise(int use_cr, unsigned n_poses, const double *poses, const double
                  const unsigned *z_step, const double *z_rb,
                  long n_obs_edges, const unsigned *pj, const unsigned *pk,
                  unsigned *t1, unsigned *t2, double *blocks);
+
+int or_round_cost(int use_cr, unsigned n_poses, const double *poses, const double *u_nu_om,
+                  double delta, double lambda, const double *mns, const unsigned *z_step,
+                  const double *z_rb, long n_obs_edges, const unsigned *pj, const unsigned *pk,
+                  double *edge_cost, double *total);
 
 long or_csr_nnz(unsigned dim, long n_edges, const unsigned *t1, const unsigned *t2);
 int or_csr_build(unsigned dim, long n_edges, const unsigned *t1, const unsigned *t2,

@@ -137,6 +137,26 @@ def linearise(g: Graph, poses, lam: float, cr: bool = True, pairs=None):
     return t1[:E], t2[:E], blocks[:E]
 
 
+def round_cost(g: Graph, poses, lam: float, cr: bool = True):
+    """(total, per-edge terms in reference edge order) of the round cost at `poses`
+    (GSLAM.c:74-87 with the intended dimensions, reset every round)."""
+    L = lib()
+    poses = np.ascontiguousarray(poses, dtype=np.float64)
+    pj, pk = obs_pairs(g.z_lm)
+    pj = np.ascontiguousarray(pj, np.uint32); pk = np.ascontiguousarray(pk, np.uint32)
+    n_obs = len(pj)
+    E = n_obs + max(g.n_poses - 1, 0)
+    per = np.zeros(max(E, 1))
+    tot = C.c_double(0.0)
+    rc = L.or_round_cost(int(cr), g.n_poses, _p(poses, C.c_double), _p(g.u, C.c_double),
+                         C.c_double(g.delta), C.c_double(lam), _p(MNS, C.c_double),
+                         _p(g.z_step, C.c_uint), _p(g.z_rb, C.c_double), C.c_long(n_obs),
+                         _p(pj, C.c_uint), _p(pk, C.c_uint), _p(per, C.c_double), C.byref(tot))
+    if rc != 0:
+        raise ValueError("observation step out of range")
+    return tot.value, per[:E]
+
+
 def csr_build(dim: int, t1, t2, blocks):
     L = lib()
     t1 = np.ascontiguousarray(t1, np.uint32); t2 = np.ascontiguousarray(t2, np.uint32)
@@ -348,6 +368,13 @@ def ref():
         R.MapEdge_create.argtypes = [C.POINTER(_MapEdge), _Z, _Z, C.POINTER(_HX), C.POINTER(C.c_double)]
         R.MapEdge_create.restype = C.POINTER(_MapEdge)
         R.vec_mean.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_uint, C.c_uint]
+        R.state_transition.argtypes = [C.POINTER(C.c_double), C.c_double, C.c_double, C.c_uint, _HX]
+        R.tra.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_uint, C.c_uint]
+        R.sub.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_uint, C.c_uint,
+                          C.POINTER(C.c_double), C.c_uint, C.c_uint]
+        R.dot.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_uint, C.c_uint,
+                          C.POINTER(C.c_double), C.c_uint, C.c_uint]
+        R.mul.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_uint, C.c_uint, C.c_double]
         _ref = R
     return _ref
 
@@ -404,6 +431,52 @@ def ref_round(g: Graph, poses, lam: float):
     R.pcg_solve_sparse(_p(dx, C.c_double), C.byref(csr), _p(xi, C.c_double), dim)
     R.free_csr(C.byref(csr))
     return t1, t2, blocks, (row_ptr, col_idx, values), xi, dx
+
+
+def ref_cost_terms(g: Graph, poses, lam: float):
+    """Per-edge cost terms from the reference's own edges and matrix functions, with the
+    dimensions GSLAM.c:74-87 meant: observation edges tra/dot/dot of their 2-element
+    hat_e with the 2x2 Omega in Omega[0..3] (ObsEdge.c:196-200), times lambda (1.0);
+    motion edges d = sub(hat_x2, state_transition(hat_x1)) (MotionEdge.c:144-148) with
+    their 3x3 Omega, times lambda."""
+    R = ref()
+    hx, us, zs = _ref_arrays(g, poses)
+    pj, _ = obs_pairs(g.z_lm)
+    E = len(pj) + g.n_poses - 1
+    edges = (_Edge * max(E, 1))()
+    lkz = (_LKZ * max(len(g.z_lm), 1))()
+    ne = C.c_uint(0); nl = C.c_uint(0)
+    R.make_edges(hx, g.n_poses, zs, len(g.z_lm), edges, C.byref(ne), lkz, C.byref(nl))
+    mns = (C.c_double * 4)(*MNS)
+    for i in range(g.n_poses - 1):
+        R.MotionEdge_create(C.byref(edges[ne.value + i]), i, i + 1, hx, us, g.delta, lam, mns)
+    E = ne.value + g.n_poses - 1
+    D = C.c_double
+    out = np.zeros(E)
+    for k in range(E):
+        ed = edges[k]
+        if k < ne.value:
+            e = (D * 2)(*ed.hat_e)
+            om = (D * 4)(*list(ed.Omega)[:4])
+            n = 2
+        else:
+            i = k - ne.value
+            nu, omega = g.u[i + 1]
+            if abs(omega) < 1e-5:
+                omega = 1e-5
+            xp = (D * 3)()
+            R.state_transition(xp, nu, omega, int(g.delta), hx[i])
+            e = (D * 3)()
+            R.sub(e, (D * 3)(*hx[i + 1].hat_x), 3, 1, xp, 3, 1)
+            om = (D * 9)(*ed.Omega)
+            n = 3
+        te = (D * n)(); t = (D * n)(); c = (D * 1)(); cl = (D * 1)()
+        R.tra(te, e, n, 1)
+        R.dot(t, te, 1, n, om, n, n)
+        R.dot(c, t, 1, n, e, n, 1)
+        R.mul(cl, c, 1, 1, ed.lam)
+        out[k] = cl[0]
+    return out
 
 
 def ref_landmark_map(g: Graph, poses):

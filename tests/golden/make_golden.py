@@ -5,8 +5,8 @@
 Each fixture holds the inputs of a reference-format log produced by the
 package's city-grid generator and the C oracle's outputs for it: edge blocks in
 both math flavours (glibc and correctly rounded), the reference CSR, xi, one
-PCG solution at the reference's settings, the poses after a short run and the
-landmark map at those poses. The
+PCG solution at the reference's settings, the poses after a short run, the
+landmark map at those poses and the per-edge round-cost terms at the logged poses. The
 oracle itself is pinned bit for bit against the reference build in
 tests/test_oracle_pin.py; these fixtures carry that pin to machines without the
 reference tree.
@@ -46,6 +46,7 @@ def make(case):
     out["dx"], _, _ = O.pcg(out["row_ptr"], out["col_idx"], out["values"], out["xi"])
     out["poses_run"], _, _ = O.run(g, lam, case["rounds"], cr=False)
     out["lm_ids"], out["lm_ms"] = O.landmark_map(g, out["poses_run"], cr=False)
+    _, out["cost_terms"] = O.round_cost(g, g.x, lam, cr=False)
     np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), **out)
 
 

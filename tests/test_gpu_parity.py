@@ -276,6 +276,44 @@ def test_landmark_map_bitwise(oracle):
         assert_bitwise(ms, ms_o, f"landmarks{n} map")
 
 
+def test_round_cost_bitwise(case, oracle):
+    """Round-cost terms (GSLAM.c:74-87 with the intended dimensions) bit for bit against
+    the oracle's correctly rounded flavour, at the logged poses and after two rounds;
+    the total within 1e-12 of the oracle's in-order sum (the device sums in blocks)."""
+    G = load_pkg()
+    name, log, lam = case
+    og = _ograph(oracle, log)
+    with G.PoseGraph.from_log(log, lam) as g:
+        for rounds_before in (0, 2):
+            for _ in range(rounds_before):
+                g.round()
+            tot, terms = g.cost(per_edge=True)
+            tot_o, terms_o = oracle.round_cost(og, g.poses, lam, cr=True)
+            assert_bitwise(terms, terms_o, f"{name} cost terms")
+            assert abs(tot - tot_o) <= 1e-12 * tot_o
+            assert g.cost() == tot
+
+
+def test_cli_cost_criterion(oracle, tmp_path):
+    """`GSLAM 0 ...`: diff = |cost - last_cost| / cost from the round's starting poses,
+    1.0 in the first round; the printed diffs follow the library's own costs."""
+    G = load_pkg()
+    log = G.synth.landmark_log(800, seed=21)
+    path = str(tmp_path / "lm800.log.txt")
+    G.synth.write_log(path, log)
+    out = subprocess.run([G.abi.CLI_PATH, "0", "0.1", "4", "0", path], capture_output=True, text=True,
+                         check=True).stdout
+    diffs = [float(l.split(":")[1]) for l in out.splitlines() if "rounds executed" in l]
+    assert diffs[0] == 1.0 and len(diffs) == 4
+    costs = []
+    with G.PoseGraph.from_log(log, 0.1) as g:
+        for _ in range(4):
+            costs.append(g.cost())
+            g.round()
+    for n in range(1, 4):
+        assert diffs[n] == abs(costs[n] - costs[n - 1]) / costs[n]
+
+
 def test_landmark_map_rejected_for_se2(oracle):
     G = load_pkg()
     cg = G.synth.city_grid(64, seed=3, block=8)

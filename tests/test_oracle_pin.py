@@ -98,6 +98,31 @@ def test_landmark_map_bitwise_vs_reference(oracle, name, lam):
         assert np.abs(ms_cr - ms).max() <= 1e-13 * max(1.0, np.abs(ms).max())
 
 
+@pytest.mark.parametrize("name,lam", [("cityTrees100.log.txt", 0.1), ("cityTrees1k.log.txt", 1.0),
+                                      ("victoria-park-100.log.txt", 0.06)])
+def test_round_cost_terms_bitwise_vs_reference(oracle, name, lam):
+    """Per-edge cost terms (GSLAM.c:74-87 with the intended dimensions) against the same
+    products formed from the reference's own edges, state_transition, tra, dot and mul;
+    at the logged poses and after two rounds. The correctly rounded flavour agrees to
+    1e-10 per term, and the total is the in-order sum of the terms."""
+    _need_ref(oracle)
+    g = oracle.read_log(ref_data(name))
+    p, _, _ = oracle.run(g, lam, 2, cr=False)
+    for poses in (g.x, p):
+        ref = oracle.ref_cost_terms(g, poses, lam)
+        tot, terms = oracle.round_cost(g, poses, lam, cr=False)
+        assert_bitwise(terms, ref, f"{name} cost terms")
+        acc = 0.0
+        for t in terms.tolist():
+            acc += t
+        assert acc == tot
+        assert (terms >= 0).all()
+        tot_cr, terms_cr = oracle.round_cost(g, poses, lam, cr=True)
+        # a one-ulp sin/cos difference is amplified by the cancellation in hat_e
+        assert (np.abs(terms_cr - terms) <= 1e-10 * terms).all()
+        assert abs(tot_cr - tot) <= 1e-12 * tot
+
+
 def test_landmark_groups_first_appearance():
     """Landmarks come in order of first appearance; members in z order."""
     import oracle as O
@@ -143,3 +168,5 @@ def test_golden_fixtures(oracle, path):
     ids, ms = oracle.landmark_map(g, p, cr=False)
     assert np.array_equal(ids, z["lm_ids"])
     assert_bitwise(ms, z["lm_ms"], "landmark map")
+    _, terms = oracle.round_cost(g, g.x, lam, cr=False)
+    assert_bitwise(terms, z["cost_terms"], "cost terms")
