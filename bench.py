@@ -48,7 +48,8 @@ def config(extra=None):
     c = {"workload": "city-grid SE(2) pose graph, N=100000, K=3 closures within 2 m, lambda=0.1; "
                      "one Gauss-Newton round with block-Jacobi PCG (tol 1e-6, max 500 iterations)",
          "n_poses": N_POSES, "lambda": LAMBDA, "pcg_tol": TOL, "pcg_max_iter": MAX_ITER,
-         "l2": "flushed between timed steps (256 MiB device write, outside the timed events)"}
+         "l2": "flushed between timed steps (256 MiB device write, outside the timed events)",
+         "round": "one CUDA graph per round (gslam_opts.round_graph), bit-identical to eager launches"}
     if extra:
         c.update(extra)
     return c
@@ -190,7 +191,8 @@ def solver_traffic(arm, iterations):
 
 def run_arm(G, torch, cg, precision, steps, warmup, flush):
     g = G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=LAMBDA,
-                             tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=precision)
+                             tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=precision,
+                             round_graph=1)
     stream = torch.cuda.ExternalStream(g.stream())
     for _ in range(warmup):
         g.round()

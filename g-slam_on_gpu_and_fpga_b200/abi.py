@@ -55,7 +55,7 @@ class Opts(C.Structure):
                 ("sell_window", C.c_int), ("threads_per_cta", C.c_int), ("ctas_per_sm", C.c_int),
                 ("angle_wrap", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
                 ("max_refine", C.c_int), ("device", C.c_int), ("barrier_timeout_ms", C.c_double),
-                ("test_absent_cta", C.c_int), ("disable_resident", C.c_int)]
+                ("test_absent_cta", C.c_int), ("disable_resident", C.c_int), ("round_graph", C.c_int)]
 
 
 class SolveStats(C.Structure):

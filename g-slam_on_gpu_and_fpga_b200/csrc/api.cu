@@ -61,6 +61,26 @@ void gslam_set_error(const char *fmt, const char *what, int code) {
         }                                                                        \
     } while (0)
 
+/* an event record that a stream capture keeps as a node of the graph (a plain record
+ * inside a capture only orders the capture) */
+static cudaError_t record_event(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t err = cudaStreamIsCapturing(st, &cs);
+    if (err != cudaSuccess) return err;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal)
+                                               : cudaEventRecord(e, st);
+}
+
+/* elapsed time between two recorded events, 0 when unavailable (leaves no error behind) */
+static float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        ms = 0.f;
+        cudaGetLastError();
+    }
+    return ms;
+}
+
 #define BAD(msg)                         \
     do {                                 \
         g_last_error = (msg);            \
@@ -307,8 +327,9 @@ int gslam_layout_ensure_fp32(DevLayout *L, cudaStream_t st) {
 }
 
 /* Runs the persistent solver on L->val / L->b4; result in L->x4 (new order). */
-int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgResult *h_res,
-                       gslam_solve_stats *stats) {
+/* everything of one solve up to the read-back of its result into h_res, without waiting
+ * (also what a captured round records) */
+static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgResult *h_res) {
     const int fused_prec = o.precision;
     if (fused_prec == GSLAM_PREC_MIXED) {
         int rc = gslam_layout_ensure_fp32(L, st);
@@ -376,17 +397,23 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
     P.halo_rows = L->halo_rows;
     P.smem_p_off = L->smem_p_off;
     tr.step("memsets");
-    CK(cudaEventRecord(L->ev0, st));
+    CK(record_event(L->ev0, st));
     if (mixed) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->mixed_smem_bytes));
     else if (resident) CK(launch_pcg_resident(st, P, grid, L->res_block, L->smem_bytes));
     else CK(launch_pcg(st, P, fused_prec, grid, L->block));
     tr.step("solver launch");
-    CK(cudaEventRecord(L->ev1, st));
+    CK(record_event(L->ev1, st));
     CK(cudaMemcpyAsync(h_res, L->res, sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    tr.step("solver wait");
+    return GSLAM_OK;
+}
+
+/* after the stream has passed the read-back: statistics, the timeout status and the FP64
+ * rerun of a stagnated mixed solve */
+static int layout_solve_finish(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgResult *h_res,
+                               gslam_solve_stats *stats) {
+    const bool mixed = o.precision == GSLAM_PREC_MIXED;
     float solve_ms = 0.f;
-    cudaEventElapsedTime(&solve_ms, L->ev0, L->ev1);
+    solve_ms = elapsed_ms(L->ev0, L->ev1);
     if (stats) {
         stats->solve_ms = solve_ms;
         stats->iterations = h_res->iterations;
@@ -417,6 +444,16 @@ int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgRe
         return rc;
     }
     return GSLAM_OK;
+}
+
+int gslam_layout_solve(DevLayout *L, cudaStream_t st, const gslam_opts &o, PcgResult *h_res,
+                       gslam_solve_stats *stats) {
+    int rc = layout_solve_enqueue(L, st, o, h_res);
+    if (rc != GSLAM_OK) return rc;
+    HostTrace tr;
+    CK(cudaStreamSynchronize(st));
+    tr.step("solver wait");
+    return layout_solve_finish(L, st, o, h_res, stats);
 }
 
 void gslam_layout_release(DevLayout *L) {
@@ -570,6 +607,8 @@ int gslam_create_se2(const gslam_se2_graph *in, const gslam_opts *opts, gslam_gr
     return GSLAM_OK;
 }
 
+static void round_graph_release(gslam_graph *g);
+
 int gslam_destroy(gslam_graph *g) {
     if (!g) return GSLAM_OK;
     if (g->st) cudaStreamSynchronize(g->st);
@@ -583,6 +622,7 @@ int gslam_destroy(gslam_graph *g) {
         if (g->batch->h_gres) cudaFreeHost(g->batch->h_gres);
         delete g->batch;
     }
+    round_graph_release(g);
     if (g->ev_round0) cudaEventDestroy(g->ev_round0);
     if (g->ev_round1) cudaEventDestroy(g->ev_round1);
     if (g->st) cudaStreamDestroy(g->st);
@@ -610,6 +650,7 @@ int gslam_set_opts(gslam_graph *g, const gslam_opts *opts) {
         g->L.grid = grid;
     }
     g->o.threads_per_cta = g->L.block;
+    round_graph_release(g); /* launch parameters may have changed */
     return GSLAM_OK;
 }
 
@@ -706,7 +747,7 @@ int gslam_update_ex(gslam_graph *g, double *diff, cudaEvent_t done) {
     launch_pose_update(g->st, g->n_poses, g->L.iperm, g->L.x4, g->d_poses, g->d_dx, g->o.angle_wrap,
                        g->d_block_sums, g->n_upd_blocks, g->d_diff);
     CK(cudaGetLastError());
-    if (done) CK(cudaEventRecord(done, g->st));
+    if (done) CK(record_event(done, g->st));
     CK(cudaMemcpyAsync(g->h_diff, g->d_diff, sizeof(double), cudaMemcpyDeviceToHost, g->st));
     CK(cudaStreamSynchronize(g->st));
     if (diff) *diff = *g->h_diff;
@@ -719,13 +760,87 @@ int gslam_get_stream(gslam_graph *g, void **stream) {
     return GSLAM_OK;
 }
 
+/* The round as one stream of work with no host wait: what the CUDA graph records.
+ * The pose update is guarded by the solver's result (a timed-out or stagnated solve
+ * leaves the poses alone; the host then decides). */
+static int round_enqueue(gslam_graph *g) {
+    CK(record_event(g->ev_round0, g->st));
+    int rc = gslam_linearise(g);
+    if (rc != GSLAM_OK) return rc;
+    rc = gslam_assemble(g);
+    if (rc != GSLAM_OK) return rc;
+    rc = layout_solve_enqueue(&g->L, g->st, g->o, g->h_res);
+    if (rc != GSLAM_OK) return rc;
+    launch_pose_update(g->st, g->n_poses, g->L.iperm, g->L.x4, g->d_poses, g->d_dx, g->o.angle_wrap,
+                       g->d_block_sums, g->n_upd_blocks, g->d_diff, g->L.res);
+    CK(cudaGetLastError());
+    CK(record_event(g->ev_round1, g->st));
+    CK(cudaMemcpyAsync(g->h_diff, g->d_diff, sizeof(double), cudaMemcpyDeviceToHost, g->st));
+    return GSLAM_OK;
+}
+
+static void round_graph_release(gslam_graph *g) {
+    if (g->round_exec) cudaGraphExecDestroy(g->round_exec);
+    g->round_exec = nullptr;
+    g->eager_rounds = 0;
+}
+
+/* captures round_enqueue on the graph's stream into an executable graph */
+static int round_graph_build(gslam_graph *g) {
+    CK(cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal));
+    const int rc = round_enqueue(g);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(g->st, &graph);
+    if (rc != GSLAM_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc == GSLAM_OK) g_last_error = std::string("round capture: ") + cudaGetErrorString(e);
+        cudaGetLastError();
+        return rc != GSLAM_OK ? rc : GSLAM_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&g->round_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        g->round_exec = nullptr;
+        g_last_error = std::string("round graph instantiate: ") + cudaGetErrorString(ei);
+        return GSLAM_ERR_CUDA;
+    }
+    return GSLAM_OK;
+}
+
+/* one round replayed from the captured graph (gslam_opts.round_graph) */
+static int round_graphed(gslam_graph *g, gslam_solve_stats *stats) {
+    if (!g->round_exec) {
+        const int rc = round_graph_build(g);
+        if (rc != GSLAM_OK) return rc;
+    }
+    CK(cudaGraphLaunch(g->round_exec, g->st));
+    CK(cudaStreamSynchronize(g->st));
+    gslam_solve_stats st;
+    memset(&st, 0, sizeof st);
+    const bool stagnated = g->o.precision == GSLAM_PREC_MIXED && !g->h_res->timeout &&
+                           g->h_res->reason == GSLAM_STOP_STAGNATION;
+    double diff = *g->h_diff;
+    int rc = layout_solve_finish(&g->L, g->st, g->o, g->h_res, &st);
+    g->last_res = *g->h_res;
+    if (rc == GSLAM_OK && stagnated) rc = gslam_update_ex(g, &diff, g->ev_round1);
+    float ms = 0.f;
+    if (rc == GSLAM_OK) ms = elapsed_ms(g->ev_round0, g->ev_round1);
+    st.diff = diff;
+    st.round_ms = ms;
+    if (stats) *stats = st;
+    return rc;
+}
+
 int gslam_round(gslam_graph *g, gslam_solve_stats *stats) {
     if (!g) BAD("null handle");
     if (!g->ev_round0) {
         CK(cudaEventCreate(&g->ev_round0));
         CK(cudaEventCreate(&g->ev_round1));
     }
-    CK(cudaEventRecord(g->ev_round0, g->st));
+    /* the first round runs eagerly: it makes every lazy allocation before a capture */
+    if (g->o.round_graph && !g->batch && g->eager_rounds > 0) return round_graphed(g, stats);
+    g->eager_rounds++;
+    CK(record_event(g->ev_round0, g->st));
     int rc = gslam_linearise(g);
     if (rc != GSLAM_OK) return rc;
     rc = gslam_assemble(g);
@@ -738,7 +853,7 @@ int gslam_round(gslam_graph *g, gslam_solve_stats *stats) {
     rc = gslam_update_ex(g, &diff, g->ev_round1);
     st.diff = diff;
     float ms = 0.f;
-    if (rc == GSLAM_OK) cudaEventElapsedTime(&ms, g->ev_round0, g->ev_round1);
+    if (rc == GSLAM_OK) ms = elapsed_ms(g->ev_round0, g->ev_round1);
     st.round_ms = ms;
     if (stats) *stats = st;
     return rc;
@@ -1149,14 +1264,14 @@ static int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve
     CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
     CK(cudaMemsetAsync(B.d_res, 0, B.n_graphs * sizeof(PcgResult), st));
     CK(cudaMemcpyAsync(B.d_active, &B.n_graphs, sizeof(int), cudaMemcpyHostToDevice, st));
-    CK(cudaEventRecord(L->ev0, st));
+    CK(record_event(L->ev0, st));
     CK(launch_pcg_batch(st, P, BP, B.grid, B.block, B.smem_bytes, false));
-    CK(cudaEventRecord(L->ev1, st));
+    CK(record_event(L->ev1, st));
     CK(cudaMemcpyAsync(g->h_res, L->res, sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(B.h_res, B.d_res, B.n_graphs * sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     float solve_ms = 0.f;
-    cudaEventElapsedTime(&solve_ms, L->ev0, L->ev1);
+    solve_ms = elapsed_ms(L->ev0, L->ev1);
     gslam_solve_stats agg;
     memset(&agg, 0, sizeof agg);
     agg.solve_ms = solve_ms;
@@ -1254,7 +1369,7 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
     BP.res = B.d_res;
     BP.active = B.d_active;
     BP.bf4 = B.d_bf4;
-    CK(cudaEventRecord(L->ev0, st));
+    CK(record_event(L->ev0, st));
     for (int step = 0; step < std::max(g->o.max_refine, 1); step++) {
         int n_active = 0, used = 0;
         for (int q = 0; q < G; q++)
@@ -1293,10 +1408,10 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
             else if (rel[q] > 0.5 * prev) { active[q] = 0; reason[q] = GSLAM_STOP_STAGNATION; stagnated = true; }
         }
     }
-    CK(cudaEventRecord(L->ev1, st));
+    CK(record_event(L->ev1, st));
     CK(cudaEventSynchronize(L->ev1));
     float solve_ms = 0.f;
-    cudaEventElapsedTime(&solve_ms, L->ev0, L->ev1);
+    solve_ms = elapsed_ms(L->ev0, L->ev1);
     if (stagnated) {
         /* the FP32 inner solves cannot resolve at least one graph: FP64 for the batch */
         gslam_solve_stats s64;
@@ -1341,7 +1456,7 @@ int gslam_batch_round(gslam_graph *g, gslam_solve_stats *per_graph) {
         CK(cudaEventCreate(&g->ev_round0));
         CK(cudaEventCreate(&g->ev_round1));
     }
-    CK(cudaEventRecord(g->ev_round0, g->st));
+    CK(record_event(g->ev_round0, g->st));
     int rc = gslam_linearise(g);
     if (rc != GSLAM_OK) return rc;
     rc = gslam_assemble(g);
@@ -1352,11 +1467,11 @@ int gslam_batch_round(gslam_graph *g, gslam_solve_stats *per_graph) {
                        g->d_block_sums, g->n_upd_blocks, g->d_diff);
     launch_batch_diff(g->st, B.n_graphs, B.d_pose_off, B.d_n_real, g->d_dx, B.d_gdiff);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(g->ev_round1, g->st));
+    CK(record_event(g->ev_round1, g->st));
     CK(cudaMemcpyAsync(B.h_gdiff, B.d_gdiff, B.n_graphs * sizeof(double), cudaMemcpyDeviceToHost, g->st));
     CK(cudaStreamSynchronize(g->st));
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, g->ev_round0, g->ev_round1);
+    ms = elapsed_ms(g->ev_round0, g->ev_round1);
     if (per_graph)
         for (int q = 0; q < B.n_graphs; q++) {
             per_graph[q].diff = B.h_gdiff[q];

@@ -116,6 +116,9 @@ struct gslam_graph {
     double *d_edge_cost = nullptr, *d_cost_blocks = nullptr, *d_cost = nullptr;
     PcgResult last_res = {};
     cudaEvent_t ev_round0 = nullptr, ev_round1 = nullptr;
+    /* gslam_opts.round_graph: the captured round and how many rounds ran eagerly */
+    cudaGraphExec_t round_exec = nullptr;
+    int eager_rounds = 0;
 };
 
 int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st, int device,

@@ -11,6 +11,7 @@
 #include <stdint.h>
 
 #include "edge_math.cuh"
+#include "gslam.h"
 #include "kernels.cuh"
 
 /* ------------------------------------------------------------------------ */
@@ -254,10 +255,16 @@ __global__ void k_diag_inv(int n_rows, const int *__restrict__ diag_slot,
  * poses[old] += x[new] (GSLAM.c:98-102) and dx[old] = x[new]; each block writes
  * the sum of dx^2 over its poses (in pose order per thread, then a fixed tree).
  */
+/* guard (may be null): the solver's result; when it timed out or stagnated the poses
+ * stay as they are (a captured round, whose host decides afterwards) */
 __global__ void k_pose_update(int n_rows, const int *__restrict__ iperm, const double *__restrict__ x4,
                               double *__restrict__ poses, double *__restrict__ dx, int wrap,
-                              double *__restrict__ block_sums) {
+                              double *__restrict__ block_sums, const PcgResult *__restrict__ guard) {
     __shared__ double sh[32];
+    if (guard && (guard->timeout || guard->reason == GSLAM_STOP_STAGNATION)) {
+        if (threadIdx.x == 0) block_sums[blockIdx.x] = 0.0;
+        return;
+    }
     double acc = 0.0;
     for (int old = blockIdx.x * blockDim.x + threadIdx.x; old < n_rows;
          old += gridDim.x * blockDim.x) {
@@ -426,8 +433,8 @@ void launch_diag_inv(cudaStream_t st, int n_rows, const int *diag_slot, const do
 
 void launch_pose_update(cudaStream_t st, int n_rows, const int *iperm, const double *x4,
                         double *poses, double *dx, int wrap, double *block_sums, int n_blocks,
-                        double *diff_out) {
-    k_pose_update<<<n_blocks, 256, 0, st>>>(n_rows, iperm, x4, poses, dx, wrap, block_sums);
+                        double *diff_out, const PcgResult *guard) {
+    k_pose_update<<<n_blocks, 256, 0, st>>>(n_rows, iperm, x4, poses, dx, wrap, block_sums, guard);
     k_finish_diff<<<1, 32, 0, st>>>(n_blocks, block_sums, 3.0 * n_rows, diff_out);
 }
 

@@ -31,9 +31,10 @@ void launch_gather_vec(cudaStream_t st, int n_rows, const int *perm, const doubl
 void launch_scatter_vec(cudaStream_t st, int n_rows, const int *perm, const double *src4, double *dst);
 void launch_diag_inv(cudaStream_t st, int n_rows, const int *diag_slot, const double *val,
                      double *dinv);
+struct PcgResult;
 void launch_pose_update(cudaStream_t st, int n_rows, const int *iperm, const double *x4,
                         double *poses, double *dx, int wrap, double *block_sums, int n_blocks,
-                        double *diff_out);
+                        double *diff_out, const PcgResult *guard = nullptr);
 
 /* ---- solver ---- */
 

@@ -65,6 +65,10 @@ typedef struct gslam_opts {
     int test_absent_cta;  /* test hook: this solver CTA never arrives at its first barrier, so
                              the others time out (checks the bounded wait); -1 = off */
     int disable_resident; /* 1: never stage the matrix in shared memory (streamed solver only) */
+    int round_graph;      /* 1: gslam_round replays the whole round (linearise, assemble,
+                             block-Jacobi, solve, pose update, read-backs) as one CUDA graph,
+                             captured at the second round; one host wait per round. Results
+                             are bit-identical to the eagerly launched round. Single graphs. */
 } gslam_opts;
 
 typedef struct gslam_solve_stats {
