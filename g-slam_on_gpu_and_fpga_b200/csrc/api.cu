@@ -299,6 +299,11 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             if (L->resident || L->mixed_ok) {
                 CK(dupload(m, st, &L->lcol, lcol));
                 CK(dupload(m, st, &L->halo_ptr, hptr));
+                /* only rows that some CTA reads as halo are published in global memory */
+                std::vector<unsigned char> exported((size_t)std::max(32 * L->n_slices, 1), 0);
+                for (int r : hrows)
+                    if (r >= 0 && (size_t)r < exported.size()) exported[(size_t)r] = 1;
+                CK(dupload(m, st, &L->row_export, exported));
                 if (hrows.empty()) hrows.push_back(0);
                 CK(dupload(m, st, &L->halo_rows, hrows));
             }
@@ -395,6 +400,7 @@ static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts 
     P.lcol = L->lcol;
     P.halo_ptr = L->halo_ptr;
     P.halo_rows = L->halo_rows;
+    P.row_export = L->row_export;
     P.smem_p_off = L->smem_p_off;
     tr.step("memsets");
     CK(record_event(L->ev0, st));

@@ -43,6 +43,7 @@ struct DevLayout {
     int *cta_slice = nullptr;      /* [res_grid + 1] */
     int64_t smem_val_cap = 0;      /* doubles staged per CTA */
     int *lcol = nullptr, *halo_ptr = nullptr, *halo_rows = nullptr; /* CTA-local columns, halo lists */
+    unsigned char *row_export = nullptr; /* rows some other CTA's halo lists */
     int64_t smem_p_off = 0;        /* staged p, after values and columns */
     size_t smem_bytes = 0;
     bool mixed_ok = false;          /* the mixed solver's shared-memory layout fits */

@@ -84,6 +84,7 @@ struct PcgParams {
     const int *lcol;       /* resident solver: per slot, CTA-local column index (own rows, then halo) */
     const int *halo_ptr;   /* resident solver: [grid + 1] halo list bounds per CTA */
     const int *halo_rows;  /* resident solver: halo rows (new row indices) */
+    const unsigned char *row_export; /* 1 for rows in another CTA's halo: only those are published */
     int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
 };
 

@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     const bool own_slice = s < s1;
     const int row = 32 * s + lane;
     const bool mine = own_slice && row < P.n_rows;
+    const bool pub = mine && __ldg(P.row_export + row); /* another CTA reads this row */
     const int len = mine ? __ldg(P.row_len + row) : 0;
     const int lslot = own_slice ? (int)(__ldg(P.slice_ptr + s) - slot0) : 0; /* local slot of (j=0) */
     /* how many of the row's blocks have their values in shared memory */
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     if (mine) {
         r = ldg3(P.b4, row);
         z = apply_dinv(P.dinv, row, r);
-        st3(P.z4, row, z);
+        if (pub) st3(P.z4, row, z);
         acc2[0] = acc2[0] + r.a * z.a; acc2[0] = acc2[0] + r.b * z.b; acc2[0] = acc2[0] + r.c * z.c;
         acc2[1] = acc2[1] + r.a * r.a; acc2[1] = acc2[1] + r.b * r.b; acc2[1] = acc2[1] + r.c * r.c;
     }
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
         V3 q = { 0.0, 0.0, 0.0 };
         if (mine) {
             pn = first ? z : V3{ z.a + beta * pn.a, z.b + beta * pn.b, z.c + beta * pn.c };
-            st3(pnew, row, pn);
+            if (pub) st3(pnew, row, pn);
             st3(sp, row - row0, pn);
         }
         if (has_h)
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
             r.a = r.a - alpha * q.a;  r.b = r.b - alpha * q.b;  r.c = r.c - alpha * q.c;
             rs[0] = rs[0] + r.a * r.a; rs[0] = rs[0] + r.b * r.b; rs[0] = rs[0] + r.c * r.c;
             z = apply_dinv(P.dinv, row, r);
-            st3(P.z4, row, z);
+            if (pub) st3(P.z4, row, z);
             rs[1] = rs[1] + r.a * z.a; rs[1] = rs[1] + r.b * z.b; rs[1] = rs[1] + r.c * z.c;
         }
         if (!grid_reduce_arrive<2, BS>(rs, P.partials, epoch, P.gs, P.spin_limit, s_red, &s_ok)) {
