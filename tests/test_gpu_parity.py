@@ -314,6 +314,63 @@ def test_cli_cost_criterion(oracle, tmp_path):
         assert diffs[n] == abs(costs[n] - costs[n - 1]) / costs[n]
 
 
+def _ref_program(oracle, name):
+    path = os.path.join(os.path.dirname(oracle.__file__), "_ref", name)
+    if not os.path.exists(path):
+        pytest.skip(f"oracle/_ref/{name} not built (needs the reference tree when building)")
+    return path
+
+
+def _rounds_and_dump(cmd, env):
+    out = subprocess.run(cmd, capture_output=True, text=True, env=env, check=True).stdout
+    diffs = [float(l.split(":")[1]) for l in out.splitlines() if "rounds executed" in l]
+    return out.splitlines(), np.array(diffs)
+
+
+def test_reference_cpu_program_on_libgslam(oracle, tmp_path):
+    """The reference CPU program (src/cpu_pcg_fp64: GSLAM.c, edges, MatrixOps.c with its own
+    pcg_solve_sparse renamed away) linked against libgslam's pcg_solve_sparse, built by
+    oracle/Makefile as INTEGRATION.md describes: the unmodified program's header and number
+    of rounds, per-round update norms and final poses within the solve's tolerance
+    (tol 1e-6 relative residual, 500 iterations: the reference's own settings)."""
+    G = load_pkg()
+    ref, dropin = _ref_program(oracle, "GSLAM"), _ref_program(oracle, "GSLAM_cpu_dropin")
+    log = G.synth.landmark_log(800, seed=21)
+    path = str(tmp_path / "lm800.txt")
+    G.synth.write_log(path, log)
+    runs = []
+    for prog in (ref, dropin):
+        dump = str(tmp_path / (os.path.basename(prog) + ".txt"))
+        lines, diffs = _rounds_and_dump([prog, "1", "0.1", "6", "1", path], dict(os.environ, POSE_DUMP_FILE=dump))
+        runs.append((lines, diffs, np.loadtxt(dump, ndmin=2)))
+    (l0, d0, p0), (l1, d1, p1) = runs
+    assert l0[:2] == l1[:2] and len(d0) == len(d1) >= 2
+    rel = np.abs(d1 - d0) / d0
+    dp = np.abs(p1[:, 1:] - p0[:, 1:]).max() / np.abs(p0[:, 1:]).max()
+    print(f"cpu drop-in: round diff rel {rel.max():.3e}, pose rel {dp:.3e}")
+    assert np.array_equal(p1[:, 0], p0[:, 0])
+    # measured on a B200: 3.8e-9 and 8.1e-10
+    assert rel.max() <= 1e-6 and dp <= 1e-6
+
+
+def test_reference_gpu_program_on_libgslam(oracle, tmp_path):
+    """The reference GPU program's main (src/gpu_pcg_fp64/GSLAM.cu with its edge files,
+    device_graph.cu and pcg.cu left out) linked against libgslam's device_graph_* /
+    device_pcg_solve: it runs end to end on the GPU and its per-round update norms follow
+    the reference CPU program's within the solve's tolerance."""
+    G = load_pkg()
+    ref, dropin = _ref_program(oracle, "GSLAM"), _ref_program(oracle, "GSLAM_gpu_dropin")
+    log = G.synth.landmark_log(800, seed=21)
+    path = str(tmp_path / "lm800.txt")
+    G.synth.write_log(path, log)
+    _, d0 = _rounds_and_dump([ref, "1", "0.1", "6", "0", path], dict(os.environ))
+    _, d1 = _rounds_and_dump([dropin, "1", "0.1", "6", "0", path], dict(os.environ))
+    rel = np.abs(d1 - d0) / d0
+    print(f"gpu drop-in: round diff rel {rel.max():.3e}")
+    assert len(d0) == len(d1) >= 2
+    assert rel.max() <= 1e-6  # measured on a B200: 2.4e-9
+
+
 def test_landmark_map_rejected_for_se2(oracle):
     G = load_pkg()
     cg = G.synth.city_grid(64, seed=3, block=8)
