@@ -530,6 +530,43 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_kernels_case(G, g, cg):
+    """Every kernel of the library at least once, for a per-kernel DRAM capture (ncu flushes
+    the caches before each captured launch, so dram bytes / duration is the kernel's HBM
+    rate): the N=100k SE(2) round kernels with 5-iteration FP64 and mixed solves, the
+    adjoint, a reference-factor graph (linearisation, round cost, landmark map), a small
+    FP64 and mixed batch, and the dense Gauss-Jordan path at n = 3072."""
+    import numpy as np
+    g.set_opts(precision=G.abi.PREC_FP64, tol=0.0, max_iter=5, angle_wrap=1)
+    g.solve()
+    g.update()
+    g.set_opts(precision=G.abi.PREC_MIXED, tol=0.0, max_iter=5, inner_max_iter=5, angle_wrap=1)
+    g.linearise()
+    g.assemble()
+    g.solve()
+    g.update()
+    g.set_opts(precision=G.abi.PREC_FP64, tol=0.0, max_iter=5, angle_wrap=1)
+    g.set_weights(LAMBDA)
+    g.adjoint(np.ones((cg.n_poses, 3)))
+    log = G.synth.landmark_log(20000, seed=3)
+    with G.PoseGraph.from_log(log, 1.0, max_iter=5) as r:
+        r.round()
+        r.cost()
+        r.landmark_map()
+    small = [G.synth.city_grid(n, seed=s) for s, n in enumerate((3000, 5000, 8000, 12000))]
+    for prec in (G.abi.PREC_FP64, G.abi.PREC_MIXED):
+        b = G.PoseGraphBatch.from_se2_list(small, LAMBDA, precision=prec, tol=0.0, max_iter=5,
+                                           inner_max_iter=5, max_refine=2, angle_wrap=1)
+        b.round_all()
+        b.close()
+    rng = np.random.default_rng(0)
+    n = 3072
+    a = rng.standard_normal((n, n)) / np.sqrt(n) + 4.0 * np.eye(n)
+    G.dense.gj_inverse(a)
+    G.dense.gj_solve(a, rng.standard_normal(n))
+    print("kernels case done", flush=True)
+
+
 def run_ncu_case(args):
     """A short, untimed solve of the bench workload for ncu captures: the solver runs
     twice on the first round's system, with 50 and then 250 iterations (tolerance 0),
@@ -543,6 +580,11 @@ def run_ncu_case(args):
                              tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=prec)
     g.linearise()
     g.assemble()
+    if args.ncu_case == "kernels":
+        run_kernels_case(G, g, cg)
+        g.close()
+        torch.cuda.synchronize()
+        return
     if args.ncu_case == "spmv":
         # two launches (warm-up + one timed) of 16 FP64 copies of the matrix
         ms = g.spmv_bench(False, reps=1, n_copies=16)
@@ -565,7 +607,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-graph batched-solve sample")
-    ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv"], default=None,
+    ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv", "kernels"], default=None,
                     help="run only two short solves of the workload (for ncu captures)")
     args = ap.parse_args()
     if args.ncu_case:

@@ -292,21 +292,30 @@ __global__ void k_pose_update(int n_rows, const int *__restrict__ iperm, const d
     }
 }
 
-/* diff = sqrt(sum of block sums in block order) / sqrt(dim) */
+/* sum of n values by one warp in a fixed order (lane-strided, then a shuffle tree): the
+ * loads of a lane are independent, so they overlap instead of one L2 round trip each */
+__device__ __forceinline__ double warp_ordered_sum(int n, const double *__restrict__ v) {
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+#pragma unroll 8
+    for (int i = lane; i < n; i += 32) s = s + v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
+    return s;
+}
+
+/* diff = sqrt(sum of the block sums) / sqrt(dim); one warp */
 __global__ void k_finish_diff(int n_blocks, const double *__restrict__ block_sums, double dim,
                               double *__restrict__ diff_out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < n_blocks; i++) s = s + block_sums[i];
-        *diff_out = sqrt(s) / sqrt(dim);
-    }
+    const double s = warp_ordered_sum(n_blocks, block_sums);
+    if (threadIdx.x == 0) *diff_out = sqrt(s) / sqrt(dim);
 }
 
 /*
  * Round cost (GSLAM.c:74-87 with the intended dimensions): one thread per edge in the
  * reference's array order (observation edges, then motion edges), the edge's term
  * computed by the linearisation's own arithmetic, stored per edge and summed per block
- * (warp tree, then warps in order); k_finish_cost adds the block sums in block order.
+ * (warp tree, then warps in order); k_finish_cost adds the block sums in a fixed order.
  */
 __global__ void k_edge_costs(int64_t n_obs_edges, int n_poses, const unsigned *__restrict__ pair_j,
                              const unsigned *__restrict__ pair_k, const unsigned *__restrict__ z_step,
@@ -350,11 +359,8 @@ __global__ void k_edge_costs(int64_t n_obs_edges, int n_poses, const unsigned *_
 }
 
 __global__ void k_finish_cost(int n_blocks, const double *__restrict__ block_sums, double *__restrict__ out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < n_blocks; i++) s = s + block_sums[i];
-        *out = s;
-    }
+    const double s = warp_ordered_sum(n_blocks, block_sums);
+    if (threadIdx.x == 0) *out = s;
 }
 
 /* ------------------------------------------------------------------------ */
