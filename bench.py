@@ -248,6 +248,28 @@ def poses_after(G, cg, precision, rounds):
     return p
 
 
+def pose_err_by_round(G, cg, checkpoints=(2, 10, 20, 40, 80)):
+    """Gauss-Newton from the initial guess with each solver (the bench's PCG settings):
+    the mixed run's poses against the FP64 run's after 2 ... 80 rounds, and each run's
+    update norm ||dx|| / sqrt(dim) in that round. Truncated solves differ per round; as the
+    iteration reaches its fixed point both runs' poses meet."""
+    snaps = {}
+    for prec in (G.abi.PREC_FP64, G.abi.PREC_MIXED):
+        g = G.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=LAMBDA,
+                                 tol=TOL, max_iter=MAX_ITER, angle_wrap=1, precision=prec, round_graph=1)
+        for k in range(1, max(checkpoints) + 1):
+            st = g.round()
+            if k in checkpoints:
+                snaps[(prec, k)] = (g.poses.copy(), st.diff)
+        g.close()
+    F, M = G.abi.PREC_FP64, G.abi.PREC_MIXED
+    return {"rounds": list(checkpoints),
+            "mixed_vs_gpu_fp64": [float(f"{pose_err_rel(snaps[(M, k)][0], snaps[(F, k)][0]):.3e}")
+                                  for k in checkpoints],
+            "update_norm_fp64": [float(f"{snaps[(F, k)][1]:.3e}") for k in checkpoints],
+            "update_norm_mixed": [float(f"{snaps[(M, k)][1]:.3e}") for k in checkpoints]}
+
+
 def cpu_baseline_sample(cg, rounds=2):
     """The oracle (reference algorithm in C, one thread) on the same workload; returns
     rounds/s, the seconds taken and the poses after `rounds` rounds."""
@@ -429,6 +451,7 @@ def run_ours(args):
     p_fp64 = poses_after(G, cg, G.abi.PREC_FP64, 2)
     p_mixed = poses_after(G, cg, G.abi.PREC_MIXED, 2)
     err = {"rounds": 2, "mixed_vs_gpu_fp64": pose_err_rel(p_mixed, p_fp64)}
+    err["by_round"] = pose_err_by_round(G, cg)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, p_oracle = cpu_baseline_sample(cg)
