@@ -330,7 +330,7 @@ def _rounds_and_dump(cmd, env):
 def test_reference_cpu_program_on_libgslam(oracle, tmp_path):
     """The reference CPU program (src/cpu_pcg_fp64: GSLAM.c, edges, MatrixOps.c with its own
     pcg_solve_sparse renamed away) linked against libgslam's pcg_solve_sparse, built by
-    oracle/Makefile as INTEGRATION.md describes: the unmodified program's header and number
+    oracle/Makefile the way a user of the reference would link it: the unmodified program's header and number
     of rounds, per-round update norms and final poses within the solve's tolerance
     (tol 1e-6 relative residual, 500 iterations: the reference's own settings)."""
     G = load_pkg()
