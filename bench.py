@@ -371,6 +371,42 @@ def spmv_sample(g, peaks):
     return out
 
 
+def scale_sample(G, torch, flush, peaks, sizes=(10000, 50000), steps=10, warmup=3):
+    """The scale sweep below the headline size: the same generator and settings at
+    N = 10,000 and 50,000 (K = 3 closures within 2 m, lambda 0.1). Per size and solver:
+    GN rounds/s over `steps` graph-captured rounds (L2 flushed between them), microseconds
+    per PCG iteration; standalone SpMV from HBM with enough matrix copies per launch to
+    exceed three L2s; the mixed run's poses against the FP64 run's after two rounds."""
+    import math
+    import statistics
+    out = {}
+    for n in sizes:
+        cg = G.synth.city_grid(n, seed=1, k_closures=3, radius=2.0, max_dtheta=0.3)
+        row = {}
+        for name, prec in (("fp64", G.abi.PREC_FP64), ("mixed", G.abi.PREC_MIXED)):
+            g, _, sz, rounds, solves, iters = run_arm(G, torch, cg, prec, steps, warmup, flush)
+            row[name] = {"gn_rounds_per_s": round(steps / (sum(rounds) * 1e-3), 2),
+                         "us_per_pcg_iteration": round(1e3 * statistics.mean(solves) / statistics.mean(iters), 3),
+                         "pcg_iterations_mean": statistics.mean(iters)}
+            if name == "fp64":
+                row["nnzb"] = sz["nnzb"]
+                spmv = {}
+                for sname, fp32 in (("fp64", False), ("fp32", True)):
+                    nbytes = g.spmv_bytes(fp32)
+                    copies = max(1, math.ceil(3 * 126e6 / nbytes))
+                    ms = g.spmv_bench(fp32, reps=5, n_copies=copies)
+                    gbs = nbytes / (ms * 1e-3) / 1e9
+                    spmv[sname] = {"achieved_gbs": round(gbs, 1), "frac": round(gbs / peaks["hbm_gbs"], 4),
+                                   "copies_per_launch": copies}
+                row["spmv_hbm"] = spmv
+            g.close()
+        row["mixed_vs_fp64"] = round(row["mixed"]["gn_rounds_per_s"] / row["fp64"]["gn_rounds_per_s"], 3)
+        row["pose_err_rel_2_rounds"] = pose_err_rel(poses_after(G, cg, G.abi.PREC_MIXED, 2),
+                                                    poses_after(G, cg, G.abi.PREC_FP64, 2))
+        out[f"N={n}"] = row
+    return out
+
+
 def c2_sample(G, rounds=50):
     """Per-round pose and residual error against the FP64 CPU oracle on the 7,120-pose
     walk with denser revisits (up to 6 closures within 3 m, ~2% of poses closing more
@@ -503,6 +539,8 @@ def run_ours(args):
     line["spmv_hbm"] = spmv_sample(results["fp64"]["g"], peaks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["per_round_vs_oracle"] = c2_sample(G)
+    if world == 1 and not args.no_scale:
+        line["scale"] = scale_sample(G, torch, flush, peaks)
     for arm in results.values():
         arm["g"].close()
     if rank == 0:
@@ -631,6 +669,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-graph batched-solve sample")
+    ap.add_argument("--no-scale", action="store_true", help="skip the N = 10k / 50k scale sample")
     ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv", "kernels"], default=None,
                     help="run only two short solves of the workload (for ncu captures)")
     args = ap.parse_args()
