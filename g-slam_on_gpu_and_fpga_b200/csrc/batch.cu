@@ -84,6 +84,23 @@ __device__ __forceinline__ TV<T> tv_spmv_row(const T *vb, const int *cb, int len
                                               T beta, bool first) {
     T q0 = 0, q1 = 0, q2 = 0;
     int j = 0;
+    /* four blocks at a time: their column and neighbour loads are in flight together (the
+     * blocks are still added one after another in ascending column order) */
+    for (; j + 3 < len; j += 4) {
+        const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
+        const int c2 = __ldg(cb + 32 * (j + 2)), c3 = __ldg(cb + 32 * (j + 3));
+        const TV<T> p0 = tv_p_of(z4, pold, c0, beta, first), p1 = tv_p_of(z4, pold, c1, beta, first);
+        const TV<T> p2 = tv_p_of(z4, pold, c2, beta, first), p3 = tv_p_of(z4, pold, c3, beta, first);
+        const TV<T> pp[4] = { p0, p1, p2, p3 };
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const T *v0 = vb + 288 * (j + u);
+            const TV<T> pu = pp[u];
+            q0 = q0 + __ldg(v0) * pu.a;       q0 = q0 + __ldg(v0 + 32) * pu.b;  q0 = q0 + __ldg(v0 + 64) * pu.c;
+            q1 = q1 + __ldg(v0 + 96) * pu.a;  q1 = q1 + __ldg(v0 + 128) * pu.b; q1 = q1 + __ldg(v0 + 160) * pu.c;
+            q2 = q2 + __ldg(v0 + 192) * pu.a; q2 = q2 + __ldg(v0 + 224) * pu.b; q2 = q2 + __ldg(v0 + 256) * pu.c;
+        }
+    }
     for (; j + 1 < len; j += 2) {
         const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
         const TV<T> p0 = tv_p_of(z4, pold, c0, beta, first), p1 = tv_p_of(z4, pold, c1, beta, first);
