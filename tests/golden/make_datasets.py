@@ -4,8 +4,11 @@ scripts' outputs, which the native gslam-data tool must reproduce byte for byte.
     python tests/golden/make_datasets.py
 
 Runs data/generate_citytrees.py (several sizes and seeds) and data/convert_slampp.py
-(on tests/golden/slampp_sample.txt, written here from a seeded generator, with gaps, a
-repeated odometry record, a blank line and a foreign record) from the reference tree.
+from the reference tree: on tests/golden/slampp_sample.txt (written here from a seeded
+generator, with gaps, a repeated odometry record, a blank line and a foreign record) and
+on tests/golden/slampp_edge_values.txt (hand-written: subnormal, largest, negative-zero,
+1e-05 / 1e16 boundary and 17-digit values, so every branch of Python's float repr is
+exercised).
 """
 import hashlib
 import json
@@ -18,8 +21,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DATA = "/root/reference/data"
-CITYTREES = [(1, 5), (80, 0), (300, 42), (1000, 7), (2500, 3), (10000, 42)]
-SLAMPP_DELTAS = ["1.0", "0.5"]
+CITYTREES = [(1, 5), (80, 0), (300, 42), (1000, 7), (2500, 3), (10000, 42), (30000, 42)]
+SLAMPP = [("slampp_sample.txt", "1.0"), ("slampp_sample.txt", "0.5"), ("slampp_edge_values.txt", "1.0")]
 
 
 def slampp_sample(path):
@@ -55,11 +58,11 @@ def main():
             subprocess.run([sys.executable, os.path.join(REF_DATA, "generate_citytrees.py"), str(n), p, str(seed)],
                            check=True, capture_output=True)
             out["citytrees"].append({"n_poses": n, "seed": seed, **digest(p)})
-        for delta in SLAMPP_DELTAS:
-            p = os.path.join(tmp, f"conv_{delta}.txt")
-            subprocess.run([sys.executable, os.path.join(REF_DATA, "convert_slampp.py"), sample, p, delta],
-                           check=True, capture_output=True)
-            out["slampp"].append({"input": "slampp_sample.txt", "delta": delta, **digest(p)})
+        for name, delta in SLAMPP:
+            p = os.path.join(tmp, f"conv_{name}_{delta}.txt")
+            r = subprocess.run([sys.executable, os.path.join(REF_DATA, "convert_slampp.py"),
+                                os.path.join(HERE, name), p, delta], check=True, capture_output=True, text=True)
+            out["slampp"].append({"input": name, "delta": delta, "summary": r.stdout.splitlines()[1], **digest(p)})
     with open(os.path.join(HERE, "datasets.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote datasets.json")
