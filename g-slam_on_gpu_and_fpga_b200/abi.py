@@ -38,7 +38,7 @@ EXPORTS = [
     "gslam_version", "gslam_last_error", "gslam_obs_edge_order", "gslam_csr_pattern",
     "pcg_solve_sparse", "device_graph_init", "device_graph_update", "device_graph_get_row_ptr",
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
-    "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_set_se2_weights", "gslam_adjoint",
+    "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_pcg_static_status", "gslam_set_se2_weights", "gslam_adjoint",
     "gslam_create_se2_batch", "gslam_batch_round", "gslam_batch_layout",
     "gslam_gj_inverse", "gslam_gj_solve", "gslam_landmark_map", "gslam_cost",
 ]
@@ -158,6 +158,7 @@ def lib() -> C.CDLL:
             "gslam_dropin_status": [],
             "gslam_pcg_solve_static": [C.c_int, VP, VP, VP, VP, VP, C.c_double, C.c_int, VP,
                                        C.POINTER(SolveStats)],
+            "gslam_pcg_static_status": [VP, C.POINTER(SolveStats)],
             "gslam_set_se2_weights": [VP, C.c_double, DP],
             "gslam_adjoint": [VP, DP, DP, DP, DP, C.POINTER(SolveStats)],
             "gslam_create_se2_batch": [C.POINTER(SE2GraphDesc), C.c_uint32, C.POINTER(Opts), C.POINTER(VP)],

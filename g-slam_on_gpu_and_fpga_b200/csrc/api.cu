@@ -428,6 +428,7 @@ static int layout_solve_finish(DevLayout *L, cudaStream_t st, const gslam_opts &
         stats->rel_residual = h_res->bnorm > 0 ? h_res->rnorm / h_res->bnorm : 0.0;
     }
     if (h_res->timeout) {
+        if (stats) stats->reason = GSLAM_STOP_TIMEOUT;
         g_last_error = "solver barrier wait timed out";
         return GSLAM_ERR_DEVICE_TIMEOUT;
     }

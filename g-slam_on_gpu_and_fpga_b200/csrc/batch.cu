@@ -340,8 +340,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B)
         }
     }
     if (timed_out && threadIdx.x == 0) {
-        P.res->timeout = 1;
-        P.res->reason = GSLAM_STOP_TIMEOUT;
+        res_mark_timeout(P.res);
     }
 }
 

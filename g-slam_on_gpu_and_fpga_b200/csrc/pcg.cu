@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64(PcgParams P) {
         acc2[1] = acc2[1] + b.a * b.a; acc2[1] = acc2[1] + b.b * b.b; acc2[1] = acc2[1] + b.c * b.c;
     }
     if (!grid_allreduce<2, BS>(acc2, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
-        if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
+        if (threadIdx.x == 0) res_mark_timeout(P.res);
         return;
     }
     double rz = acc2[0];
@@ -155,16 +155,10 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64(PcgParams P) {
         rz = rs[1];
     }
     if (reason == GSLAM_STOP_TIMEOUT && threadIdx.x == 0) {
-        P.res->timeout = 1;
-        P.res->reason = GSLAM_STOP_TIMEOUT;
+        res_mark_timeout(P.res);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && reason != GSLAM_STOP_TIMEOUT) {
-        P.res->iterations = k;
-        P.res->reason = reason;
-        P.res->refinements = 0;
-        P.res->timeout = 0;
-        P.res->rnorm = sqrt(rr);
-        P.res->bnorm = bnorm;
+        res_finish(P.res, P.gs, k, reason, 0, sqrt(rr), bnorm);
     }
 }
 

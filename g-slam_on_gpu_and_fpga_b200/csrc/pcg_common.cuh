@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "gslam.h"
 #include "kernels.cuh"
 
 /* largest dynamic shared memory the resident solver asks for (sm_100: 227 KB per block) */
@@ -69,6 +70,33 @@ __device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned epoch, long 
     if (threadIdx.x == 0) grid_barrier_t0(gs, epoch, spin_limit, s_ok);
     __syncthreads();
     return *s_ok != 0;
+}
+
+/*
+ * The solve's status record (PcgResult). The host zeroes it before every launch and
+ * the kernel only ever RAISES `timeout`: a CTA that gave up at a barrier has already
+ * arrived there, so the other CTAs can complete that barrier and finish normally while
+ * its rows of x stay behind. Block 0 must then not report success, whichever of the two
+ * writes lands last.
+ *   res_mark_timeout: any CTA that gave up (or saw another CTA give up);
+ *   res_finish:       block 0, thread 0, at the end of a solve its own CTA completed:
+ *                     counts and norms, then the reason, or a timeout when any CTA has
+ *                     raised the abort flag by then (one that gives up later raises
+ *                     `timeout` itself).
+ */
+__device__ __forceinline__ void res_mark_timeout(PcgResult *res) {
+    atomicOr(&res->timeout, 1);
+    atomicExch(&res->reason, GSLAM_STOP_TIMEOUT);
+}
+
+__device__ __forceinline__ void res_finish(PcgResult *res, const GridSync *gs, int iterations, int reason,
+                                           int refinements, double rnorm, double bnorm) {
+    res->iterations = iterations;
+    res->refinements = refinements;
+    res->rnorm = rnorm;
+    res->bnorm = bnorm;
+    res->reason = reason;
+    if (ld_relaxed_s32(&gs->abort)) res_mark_timeout(res);
 }
 
 /*

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     }
     __syncthreads();
     if (!s_ok) {
-        if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
+        if (threadIdx.x == 0) res_mark_timeout(P.res);
         return;
     }
 
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
         bb[0] = bb[0] + b.a * b.a; bb[0] = bb[0] + b.b * b.b; bb[0] = bb[0] + b.c * b.c;
     }
     if (!grid_allreduce<1, BS>(bb, P.partials, epoch, P.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
-        if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
+        if (threadIdx.x == 0) res_mark_timeout(P.res);
         return;
     }
     if (threadIdx.x == 0) {
@@ -395,16 +395,10 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
 #undef PUB_V
     /* P.x4 already holds x: stored at the start of every refinement step and after it */
     if (timed_out && threadIdx.x == 0) {
-        P.res->timeout = 1;
-        P.res->reason = GSLAM_STOP_TIMEOUT;
+        res_mark_timeout(P.res);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && !timed_out) {
-        P.res->iterations = total;
-        P.res->reason = reason;
-        P.res->refinements = outer;
-        P.res->timeout = 0;
-        P.res->rnorm = rnorm;
-        P.res->bnorm = s_sc[4];
+        res_finish(P.res, P.gs, total, reason, outer, rnorm, s_sc[4]);
     }
 }
 

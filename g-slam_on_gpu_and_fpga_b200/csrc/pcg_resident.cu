@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     }
     __syncthreads();
     if (!s_ok) {
-        if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
+        if (threadIdx.x == 0) res_mark_timeout(P.res);
         return;
     }
 
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
         acc2[1] = acc2[1] + r.a * r.a; acc2[1] = acc2[1] + r.b * r.b; acc2[1] = acc2[1] + r.c * r.c;
     }
     if (!grid_reduce_arrive<2, BS>(acc2, P.partials, epoch, P.gs, P.spin_limit, s_red, &s_ok)) {
-        if (threadIdx.x == 0) { P.res->timeout = 1; P.res->reason = GSLAM_STOP_TIMEOUT; }
+        if (threadIdx.x == 0) res_mark_timeout(P.res);
         return;
     }
     if (has_h) hz = ldcg3(P.z4, hrow);
@@ -222,16 +222,10 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     }
     if (mine) st3(P.x4, row, x);
     if (reason == GSLAM_STOP_TIMEOUT && threadIdx.x == 0) {
-        P.res->timeout = 1;
-        P.res->reason = GSLAM_STOP_TIMEOUT;
+        res_mark_timeout(P.res);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && reason != GSLAM_STOP_TIMEOUT) {
-        P.res->iterations = k;
-        P.res->reason = reason;
-        P.res->refinements = 0;
-        P.res->timeout = 0;
-        P.res->rnorm = sqrt(s_sc[1]);
-        P.res->bnorm = bnorm;
+        res_finish(P.res, P.gs, k, reason, 0, sqrt(s_sc[1]), bnorm);
     }
 }
 

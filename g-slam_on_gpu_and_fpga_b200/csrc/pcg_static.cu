@@ -57,6 +57,10 @@ static bool static_layout(unsigned char *base, int64_t nb, int grid, StaticLayou
         off += (bytes + 255) / 256 * 256;
         return p;
     };
+    /* status words first, at a fixed offset, so gslam_pcg_static_status finds them
+     * without knowing the last call's sizes */
+    L->res = (PcgResult *)take(sizeof(PcgResult));
+    L->gs = (GridSync *)take(sizeof(GridSync));
     const size_t v = 3 * (size_t)nb * sizeof(double);
     L->r = (double *)take(v);
     L->z = (double *)take(v);
@@ -65,8 +69,6 @@ static bool static_layout(unsigned char *base, int64_t nb, int grid, StaticLayou
     L->q = (double *)take(v);
     L->dinv = (double *)take(9 * (size_t)nb * sizeof(double));
     L->partials = (double *)take(8 * (size_t)grid * sizeof(double));
-    L->gs = (GridSync *)take(sizeof(GridSync));
-    L->res = (PcgResult *)take(sizeof(PcgResult));
     return off <= (size_t)GSLAM_STATIC_SCRATCH_BYTES;
 }
 
@@ -138,7 +140,7 @@ __global__ void __launch_bounds__(BS) k_pcg64_csr(CsrPcgParams P) {
         for (int c = 0; c < 3; c++) acc2[1] = acc2[1] + r[c] * r[c];
     }
     if (!grid_allreduce<2, BS>(acc2, S.partials, epoch, S.gs, P.spin_limit, s_red, s_bc, &s_ok)) {
-        if (threadIdx.x == 0) { S.res->timeout = 1; S.res->reason = GSLAM_STOP_TIMEOUT; }
+        if (threadIdx.x == 0) res_mark_timeout(S.res);
         return;
     }
     double rz = acc2[0];
@@ -199,16 +201,10 @@ __global__ void __launch_bounds__(BS) k_pcg64_csr(CsrPcgParams P) {
         rz = rs[1];
     }
     if (reason == GSLAM_STOP_TIMEOUT && threadIdx.x == 0) {
-        S.res->timeout = 1;
-        S.res->reason = GSLAM_STOP_TIMEOUT;
+        res_mark_timeout(S.res);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && reason != GSLAM_STOP_TIMEOUT) {
-        S.res->iterations = k;
-        S.res->reason = reason;
-        S.res->refinements = 0;
-        S.res->timeout = 0;
-        S.res->rnorm = sqrt(rr);
-        S.res->bnorm = bnorm;
+        res_finish(S.res, S.gs, k, reason, 0, sqrt(rr), bnorm);
     }
 }
 
@@ -221,6 +217,29 @@ struct StaticDevice {
 };
 static StaticDevice g_static_dev[GSLAM_STATIC_MAX_DEVICES];
 static std::mutex g_static_mu;
+
+/* Copies the status words of the last solve queued on this device into *stats, after
+ * the work queued on `st` so far (the solve, when the caller queued it on `st`). */
+static int static_read_status(const PcgResult *d_res, cudaStream_t st, gslam_solve_stats *stats) {
+    PcgResult h;
+    if (cudaMemcpyAsync(&h, d_res, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        gslam_set_last_error("gslam_pcg_solve_static: reading the status failed");
+        return GSLAM_ERR_CUDA;
+    }
+    stats->iterations = h.iterations;
+    stats->refinements = 0;
+    stats->reason = h.timeout ? GSLAM_STOP_TIMEOUT : h.reason;
+    stats->rel_residual = h.bnorm > 0 ? h.rnorm / h.bnorm : 0.0;
+    stats->diff = 0.0;
+    stats->solve_ms = 0.0;
+    stats->round_ms = 0.0;
+    if (h.timeout) {
+        gslam_set_last_error("gslam_pcg_solve_static: solver barrier wait timed out");
+        return GSLAM_ERR_DEVICE_TIMEOUT;
+    }
+    return GSLAM_OK;
+}
 
 extern "C" int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *d_col_idx,
                                       const double *d_values, const double *d_b, double *d_x,
@@ -302,24 +321,27 @@ extern "C" int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *
         gslam_set_last_error(cudaGetErrorString(e));
         return GSLAM_ERR_CUDA;
     }
-    if (stats) {
-        PcgResult h;
-        if (cudaMemcpyAsync(&h, P.S.res, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess) {
-            gslam_set_last_error("gslam_pcg_solve_static: reading the status failed");
-            return GSLAM_ERR_CUDA;
-        }
-        stats->iterations = h.iterations;
-        stats->refinements = 0;
-        stats->reason = h.reason;
-        stats->rel_residual = h.bnorm > 0 ? h.rnorm / h.bnorm : 0.0;
-        stats->diff = 0.0;
-        stats->solve_ms = 0.0;
-        stats->round_ms = 0.0;
-        if (h.timeout) {
-            gslam_set_last_error("gslam_pcg_solve_static: solver barrier wait timed out");
-            return GSLAM_ERR_DEVICE_TIMEOUT;
-        }
-    }
+    if (stats) return static_read_status(P.S.res, st, stats);
     return GSLAM_OK;
+}
+
+extern "C" int gslam_pcg_static_status(void *stream, gslam_solve_stats *stats) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= GSLAM_STATIC_MAX_DEVICES) {
+        gslam_set_last_error("gslam_pcg_static_status: no current CUDA device");
+        return GSLAM_ERR_NO_DEVICE;
+    }
+    unsigned char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (g_static_dev[dev].ready) base = g_static_dev[dev].base;
+    }
+    if (!base) {
+        gslam_set_last_error("gslam_pcg_static_status: no gslam_pcg_solve_static call on this device yet");
+        return GSLAM_ERR_BAD_INPUT;
+    }
+    gslam_solve_stats local;
+    StaticLayout L;
+    static_layout(base, 0, 0, &L); /* only the status words, at their fixed offset */
+    return static_read_status(L.res, (cudaStream_t)stream, stats ? stats : &local);
 }

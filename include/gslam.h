@@ -221,14 +221,25 @@ void gslam_free_log(gslam_log *log);
  * GSLAM_ERR_TOO_LARGE. It calls no cudaMalloc or cudaFree. The first call on a device
  * looks up the scratch's device address and caches it: make that first call before any
  * stream capture. All calls share the scratch, so calls that overlap on the GPU race:
- * serialise them. stats (host, may be NULL) makes the call wait for the result;
- * without it the call returns as soon as the solve is queued.
+ * serialise them. stats (host, may be NULL) makes the call wait for the result and
+ * report a timed-out solve as GSLAM_ERR_DEVICE_TIMEOUT; without it the call returns as
+ * soon as the solve is queued, and gslam_pcg_static_status reads the result later.
  */
 #define GSLAM_STATIC_SCRATCH_BYTES (4u << 20)
 #define GSLAM_STATIC_MAX_POSES 16384
 int gslam_pcg_solve_static(int dim, const int *d_row_ptr, const int *d_col_idx,
                            const double *d_values, const double *d_b, double *d_x, double tol,
                            int max_iter, void *stream, gslam_solve_stats *stats);
+/*
+ * The status of the last gslam_pcg_solve_static queued on the current device, for a
+ * caller that queued it with stats == NULL: waits for the work queued on `stream` so far
+ * (queue the read on the solve's stream, or synchronize first), then fills *stats
+ * (iterations, reason, relative residual; may be NULL) and returns GSLAM_ERR_DEVICE_TIMEOUT
+ * when a barrier wait of that solve gave up (its x is then incomplete). The status lives in
+ * the shared scratch: read it before the next call on this device overwrites it.
+ * GSLAM_ERR_BAD_INPUT when no solve has been queued on this device. Allocates nothing.
+ */
+int gslam_pcg_static_status(void *stream, gslam_solve_stats *stats);
 
 /*
  * Round cost of a reference-factor graph at its current poses: the cost that the

@@ -11,8 +11,12 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_DATA = "/root/reference/data"
-REF_DUMPS = "/root/reference/scripts/_pose_dumps_vp"
+# The reference project's tree (its data/ and scripts/ fixtures), from GSLAM_REFERENCE;
+# tests that need it skip when it is absent (e.g. on machines that only carry this repo).
+REF_ROOT = os.environ.get("GSLAM_REFERENCE", "/root/reference")
+REF_DATA = os.path.join(REF_ROOT, "data")
+REF_DUMPS = os.path.join(REF_ROOT, "scripts", "_pose_dumps_vp")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 ORACLE_DIR = os.path.join(ROOT, "oracle")

@@ -20,7 +20,7 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_DATA = "/root/reference/data"
+REF_DATA = os.path.join(os.environ.get("GSLAM_REFERENCE", "/root/reference"), "data")
 CITYTREES = [(1, 5), (80, 0), (300, 42), (1000, 7), (2500, 3), (10000, 42), (30000, 42)]
 SLAMPP = [("slampp_sample.txt", "1.0"), ("slampp_sample.txt", "0.5"), ("slampp_edge_values.txt", "1.0")]
 

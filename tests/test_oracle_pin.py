@@ -146,7 +146,8 @@ def test_victoria_park_golden_dump(oracle):
     assert_bitwise(p, ref, "Victoria Park poses")
 
 
-@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
+@pytest.mark.parametrize("path", sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                                        if not os.path.basename(p).startswith("ref_")))
 def test_golden_fixtures(oracle, path):
     """Committed oracle outputs on seeded synthetic graphs still reproduce bit for bit."""
     z = np.load(path)
@@ -170,3 +171,26 @@ def test_golden_fixtures(oracle, path):
     assert_bitwise(ms, z["lm_ms"], "landmark map")
     _, terms = oracle.round_cost(g, g.x, lam, cr=False)
     assert_bitwise(terms, z["cost_terms"], "cost terms")
+
+
+@pytest.mark.parametrize("name,fixture", [("cityTrees800.txt", "ref_citytrees800.npz"),
+                                          ("victoria-park.log.txt", "ref_victoria_park.npz")])
+def test_reference_data_fixtures(oracle, name, fixture):
+    """The committed copies of the reference's data files (tests/golden/make_ref_fixtures.py)
+    equal what the oracle's own parser reads from the reference tree, and a log written
+    back from them parses to the same values."""
+    G = load_pkg()
+    z = np.load(os.path.join(GOLDEN, fixture))
+    g = oracle.read_log(ref_data(name))
+    assert float(z["delta"]) == g.delta
+    for key, ref in (("u", g.u), ("x", g.x), ("z", g.z), ("z_lm", g.z_lm)):
+        assert np.array_equal(np.asarray(z[key]).reshape(np.shape(ref)), ref), key
+
+
+def test_vp_golden_fixture_matches_reference_dump():
+    """The committed copy of the reference's Victoria Park pose dump."""
+    dump = os.path.join(REF_DUMPS, "cpu_pcg_fp64.txt")
+    if not os.path.exists(dump):
+        pytest.skip("reference dump not present")
+    z = np.load(os.path.join(GOLDEN, "ref_vp_pcg_fp64.npz"))
+    assert_bitwise(z["poses"], np.loadtxt(dump, ndmin=2)[:, 1:4], "Victoria Park dump")

@@ -84,3 +84,25 @@ def test_static_solver_rejects_oversized_systems():
                                   C.c_void_p(d.data_ptr()), 1e-6, 10, None, None)
     assert rc == G.abi.ERR_TOO_LARGE
     assert b"16384" in L.gslam_last_error()
+
+
+def test_static_solver_status_read_back(oracle):
+    """A caller that queues the solve without waiting (stats NULL) reads its status
+    afterwards with gslam_pcg_static_status on the same stream."""
+    G = load_pkg()
+    A_ = G.abi
+    L = A_.lib()
+    rp, ci, va, xi = _system(oracle)
+    dim = len(xi)
+    dev = [torch.from_numpy(a).cuda() for a in (rp, ci, va, xi)]
+    d_x = torch.zeros(dim, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = L.gslam_pcg_solve_static(dim, *[C.c_void_p(t.data_ptr()) for t in dev], C.c_void_p(d_x.data_ptr()),
+                                  1e-6, 500, C.c_void_p(stream), None)
+    assert rc == 0, L.gslam_last_error()
+    st = A_.SolveStats()
+    rc = L.gslam_pcg_static_status(C.c_void_p(stream), C.byref(st))
+    assert rc == 0, L.gslam_last_error()
+    assert st.reason == A_.STOP_TOL and 0 < st.iterations < 500
+    assert st.rel_residual < 1e-6
+    assert L.gslam_pcg_static_status(C.c_void_p(stream), None) == 0
