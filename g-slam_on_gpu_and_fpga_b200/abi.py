@@ -40,7 +40,7 @@ EXPORTS = [
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
     "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_pcg_static_status", "gslam_set_se2_weights", "gslam_adjoint",
     "gslam_create_se2_batch", "gslam_batch_round", "gslam_batch_layout",
-    "gslam_gj_inverse", "gslam_gj_solve", "gslam_landmark_map", "gslam_cost",
+    "gslam_gj_inverse", "gslam_gj_solve", "gslam_dmma_bench", "gslam_landmark_map", "gslam_cost",
 ]
 
 
@@ -166,6 +166,7 @@ def lib() -> C.CDLL:
             "gslam_batch_layout": [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
             "gslam_gj_inverse": [C.c_int, VP, C.c_int, VP, C.POINTER(C.c_float)],
             "gslam_gj_solve": [C.c_int, VP, C.c_int, VP, VP, VP, C.POINTER(C.c_float)],
+            "gslam_dmma_bench": [C.c_int, C.c_int, DP, C.POINTER(C.c_float)],
             "gslam_landmark_map": [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), DP],
             "gslam_cost": [VP, DP, DP],
         }

@@ -32,7 +32,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC"
           "-Xcompiler", "-ffp-contract=off", "-I", CSRC, "-I", INC]
 
 LIB_SOURCES = ["structure.cpp", "kernels.cu", "pcg.cu", "pcg_resident.cu", "pcg_mixed.cu", "pcg_static.cu",
-               "adjoint.cu", "batch.cu", "gj.cu", "api.cu", "dropin.cu", "logio.cpp"]
+               "adjoint.cu", "batch.cu", "gj.cu", "api.cu", "batch_api.cu", "dropin.cu", "logio.cpp"]
 CLI_SOURCES = ["cli.cpp"]
 DATA_SOURCES = ["datasets.cpp"]
 # the dataset tool reproduces CPython's float arithmetic: C library math calls kept as calls

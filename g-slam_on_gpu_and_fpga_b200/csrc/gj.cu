@@ -259,3 +259,60 @@ int gslam_gj_solve(int n, const double *d_a, int lda, const double *d_b, double 
     cudaFree(A);
     return rc;
 }
+
+/*
+ * FP64 tensor-core throughput (the roofline of the Gauss-Jordan updates): every warp
+ * issues `reps` rounds of 8 independent m8n8k4 DMMAs (512 flops each) on register
+ * operands, so nothing but the tensor pipe limits it. The accumulators go to `out`
+ * so no MMA is dead code.
+ */
+__global__ void __launch_bounds__(256) k_dmma_peak(int reps, double *__restrict__ out) {
+    const double a = 1.0 + 1e-9 * threadIdx.x, b = 1.0 - 1e-9 * threadIdx.x;
+    double acc[8][2];
+#pragma unroll
+    for (int i = 0; i < 8; i++) { acc[i][0] = 1e-3 * i; acc[i][1] = -1e-3 * i; }
+    for (int r = 0; r < reps; r++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) dmma_8x8x4(acc[i][0], acc[i][1], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s = s + acc[i][0] + acc[i][1];
+    out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+int gslam_dmma_bench(int reps, int ctas_per_sm, double *tflops, float *ms) {
+    if (reps <= 0 || ctas_per_sm <= 0 || !tflops) { gslam_set_last_error("bad DMMA bench arguments"); return GSLAM_ERR_BAD_INPUT; }
+    int dev = 0, n_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        gslam_set_last_error("no CUDA device");
+        return GSLAM_ERR_NO_DEVICE;
+    }
+    const int grid = n_sm * ctas_per_sm, block = 256;
+    double *out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = GSLAM_ERR_CUDA;
+    float t = 0.f;
+    if (cudaMalloc(&out, (size_t)grid * block * sizeof(double)) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        gslam_set_last_error("cudaMalloc failed (DMMA bench)");
+        goto done;
+    }
+    k_dmma_peak<<<grid, block>>>(reps, out); /* warm-up */
+    cudaEventRecord(e0);
+    k_dmma_peak<<<grid, block>>>(reps, out);
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+        gslam_set_last_error("DMMA bench failed");
+        goto done;
+    }
+    *tflops = (double)grid * (block / 32) * (double)reps * 8.0 * 512.0 / (t * 1e-3) / 1e12;
+    if (ms) *ms = t;
+    rc = GSLAM_OK;
+done:
+    if (out) cudaFree(out);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return rc;
+}

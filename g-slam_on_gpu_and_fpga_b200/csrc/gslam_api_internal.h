@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "gslam.h"
@@ -136,5 +137,55 @@ int gslam_update_ex(gslam_graph *g, double *diff, cudaEvent_t done);
 /* Records an error message for gslam_last_error(). */
 void gslam_set_last_error(const char *msg);
 void gslam_set_error(const char *fmt, const char *what, int code);
+
+/* ---- helpers shared by the handle API's translation units (api.cu, batch_api.cu) ---- */
+
+/* a failing CUDA call: record it for gslam_last_error() and return GSLAM_ERR_CUDA */
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t _e = (call);                                                               \
+        if (_e != cudaSuccess) {                                                               \
+            gslam_set_last_error((std::string(#call) + ": " + cudaGetErrorString(_e)).c_str()); \
+            return GSLAM_ERR_CUDA;                                                             \
+        }                                                                                      \
+    } while (0)
+
+#define BAD(msg)                        \
+    do {                                \
+        gslam_set_last_error(msg);      \
+        return GSLAM_ERR_BAD_INPUT;     \
+    } while (0)
+
+/* device allocation owned by m (released with it) */
+template <class T>
+inline cudaError_t dalloc(DevMem &m, T **p, size_t n) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    m.ptrs.push_back(q);
+    *p = (T *)q;
+    return cudaSuccess;
+}
+
+/* device copy of a host vector, owned by m */
+template <class T>
+inline cudaError_t dupload(DevMem &m, cudaStream_t st, T **p, const std::vector<T> &v) {
+    cudaError_t e = dalloc(m, p, v.size());
+    if (e != cudaSuccess) return e;
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+/* an event record that a stream capture keeps as a node of the graph */
+cudaError_t record_event(cudaEvent_t e, cudaStream_t st);
+/* elapsed time between two recorded events, 0 when unavailable */
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b);
+/* creation steps every handle shares: options, device, stream, pinned status words */
+int common_setup(gslam_graph *g, const gslam_opts *opts);
+/* structure, layout upload and per-round buffers of a handle with edges (t1, t2) */
+int finish_setup(gslam_graph *g, const std::vector<unsigned> &t1, const std::vector<unsigned> &t2,
+                 const std::vector<int> *diag_rows = nullptr, const std::vector<int> *segments = nullptr);
+/* the batched solve behind gslam_solve / gslam_round on a batch handle (batch_api.cu) */
+int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total);
 
 #endif

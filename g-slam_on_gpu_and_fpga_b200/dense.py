@@ -34,3 +34,10 @@ def gj_solve(a: np.ndarray, b: np.ndarray):
     abi.check(abi.lib().gslam_gj_solve(n, C.c_void_p(da.data_ptr()), n, C.c_void_p(db.data_ptr()),
                                        C.c_void_p(dx.data_ptr()), None, C.byref(ms)))
     return dx.cpu().numpy(), ms.value
+
+
+def dmma_peak(reps: int = 20000, ctas_per_sm: int = 4):
+    """Measured FP64 tensor-core throughput (TFLOP/s, device ms) of the m8n8k4 DMMA."""
+    tf, ms = C.c_double(), C.c_float()
+    abi.check(abi.lib().gslam_dmma_bench(int(reps), int(ctas_per_sm), C.byref(tf), C.byref(ms)))
+    return tf.value, ms.value

@@ -298,6 +298,11 @@ int gslam_batch_layout(gslam_graph *g, uint32_t *n_graphs, uint32_t *pose_offset
  */
 int gslam_gj_inverse(int n, double *d_a, int lda, void *stream, float *ms);
 int gslam_gj_solve(int n, const double *d_a, int lda, const double *d_b, double *d_x, void *stream, float *ms);
+/* Measured FP64 tensor-core throughput (the Gauss-Jordan updates' roofline): one launch of
+ * ctas_per_sm x (SM count) CTAs of 8 warps, each warp `reps` x 8 independent m8n8k4 DMMAs on
+ * register operands, on the current device's legacy default stream; *tflops = 512 flops per
+ * DMMA / device time (*ms, may be NULL). Allocates a small output buffer. */
+int gslam_dmma_bench(int reps, int ctas_per_sm, double *tflops, float *ms);
 
 /*
  * Differentiation of a converged SE(2) graph (no counterpart in the reference, whose
