@@ -390,16 +390,39 @@ __global__ void k_add_diag(int n, const int64_t *__restrict__ slots, const doubl
     *v = *v + anchor[q];
 }
 
-/* per-graph update norm: sqrt(sum dx^2 / (3 n_real)), one CTA per graph */
-__global__ void k_batch_diff(const int *__restrict__ pose_off, const int *__restrict__ n_real,
-                             const double *__restrict__ dx, double *__restrict__ out) {
-    __shared__ double sh[32];
-    const int g = blockIdx.x;
-    const int p0 = pose_off[g], n = n_real[g];
+/*
+ * Per-graph sums of squares over the batch's vectors, spread over (chunk, graph) CTAs
+ * so a large graph does not walk its rows in one CTA: k_batch_sumsq sums chunk c of
+ * graph g (BATCH_CHUNK elements, a fixed order: thread-strided, shuffle tree, warps in
+ * order) into part[g * max_chunks + c]; k_batch_sumsq_finish adds a graph's chunk sums
+ * in chunk order (one warp per graph). Deterministic.
+ *   RESID: r4 = b4 - q4 over the graph's padded rows, sum of r^2 (the mixed batch's
+ *          FP64 refinement residual);
+ *   else:  sum of dx^2 over the graph's real poses (the update norm).
+ */
+#define BATCH_CHUNK 2048
+
+template <bool RESID>
+__global__ void __launch_bounds__(256) k_batch_sumsq(const int *__restrict__ pose_off, const int *__restrict__ n_real,
+                                                     const double *__restrict__ a, const double *__restrict__ q4,
+                                                     double *__restrict__ r4, double *__restrict__ part, int max_chunks) {
+    __shared__ double sh[8];
+    const int g = blockIdx.y, c = blockIdx.x;
+    const int p0 = pose_off[g];
+    const int n = RESID ? pose_off[g + 1] - p0 : n_real[g];
+    const int e0 = c * BATCH_CHUNK, e1 = min(3 * n, e0 + BATCH_CHUNK);
     double acc = 0.0;
-    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
-        const double d = dx[3 * (size_t)p0 + i];
-        acc = acc + d * d;
+    for (int i = e0 + (int)threadIdx.x; i < e1; i += 256) {
+        if (RESID) {
+            const int row = p0 + i / 3, comp = i - 3 * (i / 3);
+            const size_t k = 4 * (size_t)row + comp;
+            const double r = a[k] - q4[k];
+            r4[k] = r;
+            acc = acc + r * r;
+        } else {
+            const double d = a[3 * (size_t)p0 + i];
+            acc = acc + d * d;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc = acc + __shfl_down_sync(0xffffffffu, acc, o);
@@ -407,18 +430,37 @@ __global__ void k_batch_diff(const int *__restrict__ pose_off, const int *__rest
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = s + sh[w];
-        out[g] = n > 0 ? sqrt(s / (3.0 * n)) : 0.0;
+        for (int w = 0; w < 8; w++) s = s + sh[w];
+        part[(size_t)g * max_chunks + c] = s;
     }
 }
+
+__global__ void k_batch_sumsq_finish(int n_graphs, const int *__restrict__ pose_off, const int *__restrict__ n_real,
+                                     const double *__restrict__ part, int max_chunks, int diff,
+                                     double *__restrict__ out) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (g >= n_graphs) return;
+    const int n = diff ? n_real[g] : pose_off[g + 1] - pose_off[g];
+    const int nc = min(max_chunks, (3 * n + BATCH_CHUNK - 1) / BATCH_CHUNK);
+    double s = 0.0;
+    for (int c = lane; c < nc; c += 32) s = s + part[(size_t)g * max_chunks + c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[g] = diff ? (n > 0 ? sqrt(s / (3.0 * n)) : 0.0) : s;
+}
+
+int batch_max_chunks(int max_graph_rows) { return std::max(1, (3 * max_graph_rows + BATCH_CHUNK - 1) / BATCH_CHUNK); }
 
 void launch_add_diag(cudaStream_t st, int n, const int64_t *slots, const double *anchor, double *val) {
     if (n > 0) k_add_diag<<<(3 * n + 255) / 256, 256, 0, st>>>(n, slots, anchor, val);
 }
 
 void launch_batch_diff(cudaStream_t st, int n_graphs, const int *pose_off, const int *n_real, const double *dx,
-                       double *out) {
-    if (n_graphs > 0) k_batch_diff<<<n_graphs, 256, 0, st>>>(pose_off, n_real, dx, out);
+                       double *out, double *part, int max_chunks) {
+    if (n_graphs <= 0) return;
+    k_batch_sumsq<false><<<dim3(max_chunks, n_graphs), 256, 0, st>>>(pose_off, n_real, dx, nullptr, nullptr, part,
+                                                                     max_chunks);
+    k_batch_sumsq_finish<<<(n_graphs + 7) / 8, 256, 0, st>>>(n_graphs, pose_off, n_real, part, max_chunks, 1, out);
 }
 
 /* ---- the mixed batch's refinement steps (FP64) ---- */
@@ -445,30 +487,6 @@ __global__ void k_batch_add_x(int n_rows, const float *__restrict__ xf4, double 
     x[2] = x[2] + (double)d.z;
 }
 
-/* r4 = b4 - q4 (q4 = A x) and each graph's ||r||^2, one CTA per graph */
-__global__ void k_batch_resid(const int *__restrict__ pose_off, const double *__restrict__ b4,
-                              const double *__restrict__ q4, double *__restrict__ r4, double *__restrict__ out) {
-    __shared__ double sh[32];
-    const int g = blockIdx.x;
-    const int r0 = pose_off[g], r1 = pose_off[g + 1];
-    double acc = 0.0;
-    for (int i = 3 * r0 + threadIdx.x; i < 3 * r1; i += blockDim.x) {
-        const int row = i / 3, c = i - 3 * row;
-        const double r = b4[4 * (size_t)row + c] - q4[4 * (size_t)row + c];
-        r4[4 * (size_t)row + c] = r;
-        acc = acc + r * r;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc = acc + __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = s + sh[w];
-        out[g] = s;
-    }
-}
-
 void launch_batch_rhs32(cudaStream_t st, int n_rows, const int *slice_graph, const int *active, const double *r4,
                         float *bf4) {
     k_batch_rhs32<<<(n_rows + 255) / 256, 256, 0, st>>>(n_rows, slice_graph, active, r4, bf4);
@@ -479,6 +497,8 @@ void launch_batch_add_x(cudaStream_t st, int n_rows, const float *xf4, double *x
 }
 
 void launch_batch_resid(cudaStream_t st, int n_graphs, const int *pose_off, const double *b4, const double *q4,
-                        double *r4, double *out) {
-    k_batch_resid<<<n_graphs, 256, 0, st>>>(pose_off, b4, q4, r4, out);
+                        double *r4, double *out, double *part, int max_chunks) {
+    if (n_graphs <= 0) return;
+    k_batch_sumsq<true><<<dim3(max_chunks, n_graphs), 256, 0, st>>>(pose_off, nullptr, b4, q4, r4, part, max_chunks);
+    k_batch_sumsq_finish<<<(n_graphs + 7) / 8, 256, 0, st>>>(n_graphs, pose_off, nullptr, part, max_chunks, 0, out);
 }

@@ -153,6 +153,7 @@ int gslam_create_se2_batch(const gslam_se2_graph *graphs, uint32_t n_graphs, con
         const int padded = (int)((in.n_poses + 31) / 32 * 32);
         B.pose_off[q + 1] = off + padded;
         B.n_real[q] = (int)in.n_poses;
+        B.max_chunks = std::max(B.max_chunks, batch_max_chunks(padded));
         segments.push_back(off);
         for (uint32_t e = 0; e < in.n_edges; e++) {
             t1.push_back((unsigned)off + in.edge_i[e]);
@@ -189,6 +190,7 @@ int gslam_create_se2_batch(const gslam_se2_graph *graphs, uint32_t n_graphs, con
         dupload(m, g->st, &B.d_pose_off, B.pose_off) != cudaSuccess ||
         dupload(m, g->st, &B.d_n_real, B.n_real) != cudaSuccess ||
         dalloc(m, &B.d_gdiff, (size_t)n_graphs) != cudaSuccess || dalloc(m, &B.d_res, (size_t)n_graphs) != cudaSuccess ||
+        dalloc(m, &B.d_chunk_part, (size_t)n_graphs * B.max_chunks) != cudaSuccess ||
         dalloc(m, &B.d_active, 1) != cudaSuccess ||
         cudaMallocHost(&B.h_res, n_graphs * sizeof(PcgResult)) != cudaSuccess ||
         cudaMallocHost(&B.h_gdiff, n_graphs * sizeof(double)) != cudaSuccess) {
@@ -315,7 +317,7 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
     /* x = 0; r = b - A 0 = b with per-graph ||b|| */
     CK(cudaMemsetAsync(L->x4, 0, 4 * 32 * (size_t)L->n_slices * sizeof(double), st));
     CK(cudaMemsetAsync(L->q4, 0, 4 * 32 * (size_t)L->n_slices * sizeof(double), st));
-    launch_batch_resid(st, G, B.d_pose_off, L->b4, L->q4, L->r4, B.d_gres);
+    launch_batch_resid(st, G, B.d_pose_off, L->b4, L->q4, L->r4, B.d_gres, B.d_chunk_part, B.max_chunks);
     CK(cudaMemcpyAsync(B.h_gres, B.d_gres, G * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     std::vector<double> bnorm(G), rel(G, 1.0);
@@ -374,7 +376,7 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
         CK(launch_pcg_batch(st, P, BP, B.grid, B.block, B.smem_bytes, true));
         launch_batch_add_x(st, L->n_rows, L->f[0], L->x4);
         launch_spmv64(st, L->n_rows, L->n_slices, L->slice_ptr, L->row_len, L->col, L->val, L->x4, L->q4);
-        launch_batch_resid(st, G, B.d_pose_off, L->b4, L->q4, L->r4, B.d_gres);
+        launch_batch_resid(st, G, B.d_pose_off, L->b4, L->q4, L->r4, B.d_gres, B.d_chunk_part, B.max_chunks);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(g->h_res, L->res, sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(B.h_res, B.d_res, G * sizeof(PcgResult), cudaMemcpyDeviceToHost, st));
@@ -452,7 +454,7 @@ int gslam_batch_round(gslam_graph *g, gslam_solve_stats *per_graph) {
     if (rc != GSLAM_OK) return rc;
     launch_pose_update(g->st, g->n_poses, g->L.iperm, g->L.x4, g->d_poses, g->d_dx, g->o.angle_wrap,
                        g->d_block_sums, g->n_upd_blocks, g->d_diff);
-    launch_batch_diff(g->st, B.n_graphs, B.d_pose_off, B.d_n_real, g->d_dx, B.d_gdiff);
+    launch_batch_diff(g->st, B.n_graphs, B.d_pose_off, B.d_n_real, g->d_dx, B.d_gdiff, B.d_chunk_part, B.max_chunks);
     CK(cudaGetLastError());
     CK(record_event(g->ev_round1, g->st));
     CK(cudaMemcpyAsync(B.h_gdiff, B.d_gdiff, B.n_graphs * sizeof(double), cudaMemcpyDeviceToHost, g->st));

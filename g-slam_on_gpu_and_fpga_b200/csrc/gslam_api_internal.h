@@ -79,6 +79,9 @@ struct BatchState {
     float *d_bf4 = nullptr;
     int *d_gactive = nullptr;
     double *d_gres = nullptr, *h_gres = nullptr;
+    /* chunk sums of the per-graph norm kernels */
+    double *d_chunk_part = nullptr;
+    int max_chunks = 1;
 };
 
 struct gslam_graph {

@@ -132,10 +132,14 @@ void launch_add_diag(cudaStream_t st, int n, const int64_t *slots, const double 
 void launch_batch_rhs32(cudaStream_t st, int n_rows, const int *slice_graph, const int *active, const double *r4,
                         float *bf4);
 void launch_batch_add_x(cudaStream_t st, int n_rows, const float *xf4, double *x4);
+/* per-graph ||b - q||^2 (writing r4 = b4 - q4) and update norms, spread over (chunk, graph)
+ * CTAs; part holds n_graphs x max_chunks chunk sums, max_chunks = batch_max_chunks(rows of
+ * the largest padded graph) */
 void launch_batch_resid(cudaStream_t st, int n_graphs, const int *pose_off, const double *b4, const double *q4,
-                        double *r4, double *out);
+                        double *r4, double *out, double *part, int max_chunks);
 void launch_batch_diff(cudaStream_t st, int n_graphs, const int *pose_off, const int *n_real, const double *dx,
-                       double *out);
+                       double *out, double *part, int max_chunks);
+int batch_max_chunks(int max_graph_rows);
 
 /* Cooperative launch of the persistent solver; returns the CUDA error. */
 cudaError_t launch_pcg(cudaStream_t st, const PcgParams &p, int precision, int grid, int block);

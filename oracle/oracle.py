@@ -519,3 +519,30 @@ def ref_run_binary(log_path: str, lam: float, rounds: int, dump_path: str, use_d
                          capture_output=True, text=True, env=env, check=True)
     poses = np.loadtxt(dump_path, dtype=np.float64, ndmin=2)[:, 1:4]
     return out.stdout, poses
+
+
+def gn_fixed_point(poses, ei, ej, meas, log_w, lam: float, anchor: float = 1e6, max_rounds: int = 40,
+                   stop: float = 1e-9):
+    """The Gauss-Newton fixed point of an SE(2) graph with DIRECT FP64 solves: the edge
+    blocks and the assembled Omega / xi of the C restatement (se2_linearise,
+    csr_build_anchor), each round's Omega dx = xi solved by a sparse LU factorisation
+    (scipy's SuperLU, COLAMD ordering) instead of PCG, angles wrapped in the update.
+    Stops when ||dx|| / sqrt(dim) < stop or after max_rounds. At the fixed point the
+    result does not depend on the linear solver, so this is the reference for where any
+    converged Gauss-Newton run must end. Returns (poses, per-round update norms)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    p = np.array(poses, np.float64).reshape(-1, 3)
+    dim = 3 * p.shape[0]
+    diffs = []
+    for _ in range(max_rounds):
+        blocks, _ = se2_linearise(p, ei, ej, meas, log_w, lam)
+        rp, ci, va, xi = csr_build_anchor(dim, ei, ej, blocks, anchor)
+        A = sp.csr_matrix((va, ci, rp), shape=(dim, dim)).tocsc()
+        dx = spl.spsolve(A, xi, permc_spec="COLAMD")
+        p = p + dx.reshape(-1, 3)
+        p[:, 2] = (p[:, 2] + np.pi) % (2 * np.pi) - np.pi
+        diffs.append(float(np.linalg.norm(dx) / np.sqrt(dim)))
+        if diffs[-1] < stop:
+            break
+    return p, diffs

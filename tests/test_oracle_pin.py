@@ -194,3 +194,17 @@ def test_vp_golden_fixture_matches_reference_dump():
         pytest.skip("reference dump not present")
     z = np.load(os.path.join(GOLDEN, "ref_vp_pcg_fp64.npz"))
     assert_bitwise(z["poses"], np.loadtxt(dump, ndmin=2)[:, 1:4], "Victoria Park dump")
+
+
+def test_gn_fixed_point_direct(oracle):
+    """The oracle's direct-solve Gauss-Newton (the fixed point converged runs are held to)
+    stops at a stationary point: xi there is many orders below its starting size."""
+    G = load_pkg()
+    cg = G.synth.city_grid(300, seed=4)
+    p, diffs = oracle.gn_fixed_point(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1)
+    assert diffs[-1] < 1e-9 and len(diffs) < 40
+    xi_norm = []
+    for q in (cg.init, p):
+        blocks, _ = oracle.se2_linearise(q, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1)
+        xi_norm.append(np.linalg.norm(oracle.csr_build_anchor(3 * cg.n_poses, cg.edge_i, cg.edge_j, blocks, 1e6)[3]))
+    assert xi_norm[1] < 1e-8 * xi_norm[0]
