@@ -200,7 +200,8 @@ def test_gn_fixed_point_direct(oracle):
     """The oracle's direct-solve Gauss-Newton (the fixed point converged runs are held to)
     stops at a stationary point: xi there is many orders below its starting size."""
     G = load_pkg()
-    cg = G.synth.city_grid(300, seed=4)
+    cg = G.synth.city_grid(400, seed=3, block=5, k_closures=6, radius=3.0)
+    assert cg.n_closures > 0
     p, diffs = oracle.gn_fixed_point(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1)
     assert diffs[-1] < 1e-9 and len(diffs) < 40
     xi_norm = []
