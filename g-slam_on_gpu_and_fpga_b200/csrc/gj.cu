@@ -8,7 +8,7 @@
  * the iterative solvers. Here the same elimination (no pivoting) is blocked by
  * b = 64 columns; step k with K = [64k, 64k + 64):
  *   U = A[:, K] (copy of the old block column), P = A[K, K]^-1 (one CTA, unblocked
- *   in-place Gauss-Jordan in shared memory),
+ *   in-place Gauss-Jordan with the block in registers),
  *   A[K, J] = P A[K, J]                 for J != K   (row panel)
  *   A[I, J] = A[I, J] - U[I] A[K, J]    for I, J != K (trailing update, rank 64)
  *   A[I, K] = -U[I] P                   for I != K,   A[K, K] = P.
@@ -75,28 +75,58 @@ __global__ void k_gj_copy_col(int n, const double *__restrict__ A, int k0, doubl
     U[t] = A[(size_t)r * n + k0 + c];
 }
 
-/* P = inv(U[K, :]) by in-place Gauss-Jordan without pivoting (one CTA) */
-__global__ void k_gj_diag(const double *__restrict__ U, int k0, double *__restrict__ P) {
-    __shared__ double T[GJ_B][GJ_B + 1];
-    __shared__ double s_row[GJ_B], s_col[GJ_B];
-    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) T[t >> 6][t & 63] = U[(size_t)(k0 + (t >> 6)) * GJ_B + (t & 63)];
-    __syncthreads();
-    for (int i = 0; i < GJ_B; i++) {
-        const double p = 1.0 / T[i][i];
-        if (threadIdx.x < GJ_B) {
-            const int j = threadIdx.x;
-            s_row[j] = (j == i ? 1.0 : T[i][j]) * p; /* new pivot row */
-            s_col[j] = T[j][i];                      /* old pivot column */
+/*
+ * P = inv(U[K, :]) by in-place Gauss-Jordan without pivoting, one CTA of 256 threads
+ * with the 64 x 64 block in registers: thread t owns row r = t / 4 and columns
+ * [16 g, 16 g + 16), g = t % 4, so a warp holds 8 whole rows. Pivot step i: every
+ * thread takes f = T[r][i] from the lane of its row that owns column i (a shuffle inside
+ * the row's four lanes); the four threads of row i form the new pivot row
+ * (T[i][i] -> 1, then every entry times p = 1 / T[i][i]) and write it to one of two
+ * shared buffers; one CTA barrier; every other row does T[r][c] -= f * pivot[c] with
+ * T[r][i] -> 0 first. Per element the same operations as the unblocked elimination
+ * (src/cpu_pcg_fp64/MatrixOps.c:29-91: the ratio, then the subtraction). The two
+ * buffers alternate, so one barrier per step suffices: the buffer written at step i was
+ * last read at step i - 2, before every thread passed step i - 1's barrier.
+ */
+__global__ void __launch_bounds__(256) k_gj_diag(const double *__restrict__ U, int k0, double *__restrict__ P) {
+    __shared__ __align__(16) double s_prow[2][GJ_B];
+    const int t = threadIdx.x, r = t >> 2, g = t & 3;
+    const int row_lane0 = (t & 31) & ~3; /* this row's first lane in the warp */
+    double T[16];
+    const double *src = U + (size_t)(k0 + r) * GJ_B + 16 * g;
+#pragma unroll
+    for (int j = 0; j < 16; j++) T[j] = src[j];
+    for (int gi = 0; gi < 4; gi++) {
+#pragma unroll
+        for (int jj = 0; jj < 16; jj++) {
+            const int i = 16 * gi + jj, buf = i & 1;
+            const double f = __shfl_sync(0xffffffffu, T[jj], row_lane0 + gi);
+            if (r == i) {
+                const double p = 1.0 / f;
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const double v = (16 * g + j == i) ? 1.0 : T[j];
+                    T[j] = v * p;
+                    s_prow[buf][16 * g + j] = T[j];
+                }
+            }
+            __syncthreads();
+            if (r != i) {
+                const double2 *pr = reinterpret_cast<const double2 *>(&s_prow[buf][16 * g]);
+#pragma unroll
+                for (int j = 0; j < 16; j += 2) {
+                    const double2 q = pr[j >> 1];
+                    const double v0 = (16 * g + j == i) ? 0.0 : T[j];
+                    const double v1 = (16 * g + j + 1 == i) ? 0.0 : T[j + 1];
+                    T[j] = v0 - f * q.x;
+                    T[j + 1] = v1 - f * q.y;
+                }
+            }
         }
-        __syncthreads();
-        for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) {
-            const int r = t >> 6, c = t & 63;
-            if (r == i) T[r][c] = s_row[c];
-            else T[r][c] = (c == i ? 0.0 : T[r][c]) - s_col[r] * s_row[c];
-        }
-        __syncthreads();
     }
-    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) P[t] = T[t >> 6][t & 63];
+    double *dst = P + (size_t)r * GJ_B + 16 * g;
+#pragma unroll
+    for (int j = 0; j < 16; j++) dst[j] = T[j];
 }
 
 /* row panel: A[K, J] = P A[K, J] for every 64-column tile J != K (one CTA per tile) */
@@ -202,7 +232,7 @@ static int gj_run(int m, double *d_a, cudaStream_t st, double *scratch) {
     for (int k = 0; k < nt; k++) {
         const int k0 = GJ_B * k;
         k_gj_copy_col<<<(m * GJ_B + 255) / 256, 256, 0, st>>>(m, d_a, k0, U);
-        k_gj_diag<<<1, 1024, 0, st>>>(U, k0, P);
+        k_gj_diag<<<1, 256, 0, st>>>(U, k0, P);
         k_gj_row_panel<<<nt, 128, smem, st>>>(m, d_a, k0, P);
         k_gj_update<<<dim3(nt, nt), 128, smem, st>>>(m, d_a, k0, U, P);
     }
