@@ -12,7 +12,8 @@
  *   A[K, J] = P A[K, J]                 for J != K   (row panel)
  *   A[I, J] = A[I, J] - U[I] A[K, J]    for I, J != K (trailing update, rank 64)
  *   A[I, K] = -U[I] P                   for I != K,   A[K, K] = P.
- * After the last step A holds A^-1. The row panel, trailing update and column panel
+ * After the last step A holds A^-1. The next step's copy U of its block column is written
+ * by this step's row panel and trailing update as they produce it (no copy launch). The row panel, trailing update and column panel
  * are 64x64-tile GEMMs with K = 64 on mma.sync.m8n8k4 FP64 (DMMA): one CTA per
  * output tile, both 64x64 operand tiles staged in shared memory (rows padded to 68
  * doubles against bank conflicts), four warps of 32x32 each (4 x 4 m8n8 tiles).
@@ -129,13 +130,16 @@ __global__ void __launch_bounds__(256) k_gj_diag(const double *__restrict__ U, i
     for (int j = 0; j < 16; j++) dst[j] = T[j];
 }
 
-/* row panel: A[K, J] = P A[K, J] for every 64-column tile J != K (one CTA per tile) */
+/* row panel: A[K, J] = P A[K, J] for every 64-column tile J != K (one CTA per tile); the
+ * tile of the next pivot column (J = K + 1) also goes to Un, that step's copy of its block
+ * column (rows K; the other rows come from the trailing update) */
 __global__ void __launch_bounds__(128) k_gj_row_panel(int n, double *__restrict__ A, int k0,
-                                                      const double *__restrict__ P) {
+                                                      const double *__restrict__ P, double *__restrict__ Un) {
     extern __shared__ __align__(16) double sm[];
     double *sA = sm, *sB = sm + GJ_B * GJ_LD;
     const int tj = blockIdx.x;
     if (64 * tj == k0) return;
+    const bool next = (64 * tj == k0 + GJ_B);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wm = warp >> 1, wn = warp & 1;
     load_tile(sA, P, GJ_B);
     load_tile(sB, A + (size_t)k0 * n + 64 * tj, n);
@@ -151,14 +155,17 @@ __global__ void __launch_bounds__(128) k_gj_row_panel(int n, double *__restrict_
             double *dst = A + (size_t)(k0 + r) * n + 64 * tj + c;
             dst[0] = acc[i][j][0];
             dst[1] = acc[i][j][1];
+            if (next) *reinterpret_cast<double2 *>(Un + (size_t)(k0 + r) * GJ_B + c) = make_double2(acc[i][j][0], acc[i][j][1]);
         }
 }
 
 /* trailing update and column panel, one CTA per 64x64 tile (I, J), I != K:
  *   J != K: A[I, J] -= U[I] A[K, J];   J == K: A[I, K] = -U[I] P.
- * Tile (K, K) writes P. */
+ * Tile (K, K) writes P. The old A[I, J] is loaded into registers before the operand tiles
+ * (its latency overlaps theirs); tiles of the next pivot column also go to Un. */
 __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A, int k0,
-                                                   const double *__restrict__ U, const double *__restrict__ P) {
+                                                   const double *__restrict__ U, const double *__restrict__ P,
+                                                   double *__restrict__ Un) {
     extern __shared__ __align__(16) double sm[];
     double *sA = sm, *sB = sm + GJ_B * GJ_LD;
     const int ti = blockIdx.y, tj = blockIdx.x;
@@ -170,7 +177,19 @@ __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A
                 A[(size_t)(k0 + (t >> 6)) * n + k0 + (t & 63)] = P[t];
         return;
     }
-    const bool colp = (64 * tj == k0);
+    const bool colp = (64 * tj == k0), next = (64 * tj == k0 + GJ_B);
+    double old[4][4][2];
+    if (!colp) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int r = 32 * wm + 8 * i + gid, c = 32 * wn + 8 * j + 2 * tig;
+                const double2 v = *reinterpret_cast<const double2 *>(A + (size_t)(64 * ti + r) * n + 64 * tj + c);
+                old[i][j][0] = v.x;
+                old[i][j][1] = v.y;
+            }
+    }
     load_tile(sA, U + (size_t)(64 * ti) * GJ_B, GJ_B);
     load_tile(sB, colp ? P : A + (size_t)k0 * n + 64 * tj, colp ? GJ_B : n);
     __syncthreads();
@@ -181,14 +200,11 @@ __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int r = 32 * wm + 8 * i + gid, c = 32 * wn + 8 * j + 2 * tig;
-            double *dst = A + (size_t)(64 * ti + r) * n + 64 * tj + c;
-            if (colp) {
-                dst[0] = -acc[i][j][0];
-                dst[1] = -acc[i][j][1];
-            } else {
-                dst[0] = dst[0] - acc[i][j][0];
-                dst[1] = dst[1] - acc[i][j][1];
-            }
+            double2 v;
+            if (colp) v = make_double2(-acc[i][j][0], -acc[i][j][1]);
+            else v = make_double2(old[i][j][0] - acc[i][j][0], old[i][j][1] - acc[i][j][1]);
+            *reinterpret_cast<double2 *>(A + (size_t)(64 * ti + r) * n + 64 * tj + c) = v;
+            if (next) *reinterpret_cast<double2 *>(Un + (size_t)(64 * ti + r) * GJ_B + c) = v;
         }
 }
 
@@ -219,8 +235,11 @@ __global__ void k_gemv(int m, const double *__restrict__ A, const double *__rest
 }
 
 static int gj_run(int m, double *d_a, cudaStream_t st, double *scratch) {
-    /* scratch: U (m x 64) then P (64 x 64) */
-    double *U = scratch, *P = scratch + (size_t)m * GJ_B;
+    /* scratch: two copies of a block column (m x 64 each, this step's and the next's) then
+     * P (64 x 64); the first step's copy is made here, every later one by the previous
+     * step's row panel and trailing update */
+    double *Ub[2] = { scratch, scratch + (size_t)m * GJ_B };
+    double *P = scratch + 2 * (size_t)m * GJ_B;
     const size_t smem = 2 * GJ_B * GJ_LD * sizeof(double);
     static bool attr = false;
     if (!attr) {
@@ -229,12 +248,13 @@ static int gj_run(int m, double *d_a, cudaStream_t st, double *scratch) {
         attr = true;
     }
     const int nt = m / GJ_B;
+    k_gj_copy_col<<<(m * GJ_B + 255) / 256, 256, 0, st>>>(m, d_a, 0, Ub[0]);
     for (int k = 0; k < nt; k++) {
         const int k0 = GJ_B * k;
-        k_gj_copy_col<<<(m * GJ_B + 255) / 256, 256, 0, st>>>(m, d_a, k0, U);
+        double *U = Ub[k & 1], *Un = Ub[(k + 1) & 1];
         k_gj_diag<<<1, 256, 0, st>>>(U, k0, P);
-        k_gj_row_panel<<<nt, 128, smem, st>>>(m, d_a, k0, P);
-        k_gj_update<<<dim3(nt, nt), 128, smem, st>>>(m, d_a, k0, U, P);
+        k_gj_row_panel<<<nt, 128, smem, st>>>(m, d_a, k0, P, Un);
+        k_gj_update<<<dim3(nt, nt), 128, smem, st>>>(m, d_a, k0, U, P, Un);
     }
     return cudaGetLastError() == cudaSuccess ? GSLAM_OK : GSLAM_ERR_CUDA;
 }
@@ -247,7 +267,7 @@ int gslam_gj_inverse(int n, double *d_a, int lda, void *stream, float *ms) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int rc = GSLAM_ERR_CUDA;
     if (cudaMalloc(&B, (size_t)m * m * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&scratch, ((size_t)m * GJ_B + GJ_B * GJ_B) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&scratch, (2 * (size_t)m * GJ_B + GJ_B * GJ_B) * sizeof(double)) != cudaSuccess ||
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         gslam_set_last_error("cudaMalloc failed (dense inverse)");
         goto done;
