@@ -46,7 +46,7 @@ LAMBDA = 0.1
 TOL, MAX_ITER = 1e-6, 500          # the reference's per-round PCG settings (MatrixOps.c:345-347)
 POSE_ERR_BAR = 1e-6                # the metric's accuracy bar (relative pose error vs the FP64 oracle)
 FIXED_POINT = 1e-6                 # ||dx|| / sqrt(dim) below this: Gauss-Newton at its fixed point
-CONV_N, CONV_TOL, CONV_MAX_ITER = 20000, 1e-10, 400000   # the converged block
+CONV_SIZES, CONV_TOL, CONV_MAX_ITER = (20000, 50000), 1e-8, 400000   # the converged block
 METRIC = "GN iters/s at N=100k: mixed vs FP64 PCG on B200 (pose err<=1e-6); SpMV HBM GB/s"
 UNIT = "GN iters/s"
 
@@ -294,11 +294,11 @@ def cpu_model():
         return {"model": None, "cpus": None}
 
 
-def converged_sample(G, torch, flush, n=CONV_N, steps=20, warmup=2):
+def converged_sample(G, torch, flush, n, steps=20, warmup=1):
     """Gauss-Newton to its fixed point with converged solves, at the largest size where
     block-Jacobi PCG gets there in a bench's time (at N = 100,000 even 200,000 iterations
     per round leave relative residuals up to 3e-2 and the update norm above 0.5 after 25
-    rounds, where direct solves settle in 13): the same generator at N = CONV_N, PCG to
+    rounds, where direct solves settle in 13): the same generator at N = n, PCG to
     CONV_TOL per round (iterations capped at CONV_MAX_ITER), up to `steps` rounds from
     the initial guess, stopping when ||dx|| / sqrt(dim) < FIXED_POINT. Both solvers;
     final poses against each other and against the oracle's direct-solve fixed point
@@ -679,7 +679,7 @@ def run_ours(args):
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if world == 1 and not args.no_scale:
-        line["converged"] = converged_sample(G, torch, flush)
+        line["converged"] = {f"N={n}": converged_sample(G, torch, flush, n) for n in CONV_SIZES}
         line["scale"] = scale_sample(G, torch, flush, peaks)
     if not args.no_batch:
         line["batch"] = batch_sample(G, torch, 3, world, rank, dist)

@@ -106,3 +106,95 @@ def position_loss(poses, target):
     g = np.zeros_like(poses)
     g[:, :2] = 2.0 * d
     return float((d ** 2).sum()), g
+
+
+# ---- sparse forms of the same reference (scipy SuperLU), for sizes a dense solve cannot hold ----
+
+def system_sparse(poses, ei, ej, meas, log_w, lam, anchor, exact=False):
+    """system() with Omega (or the exact Hessian) as a scipy CSC matrix."""
+    import scipy.sparse as sp
+    n = poses.shape[0]
+    e, Ji, Jj, (c, s, dx, dy) = residuals(poses, ei, ej, meas)
+    L = lam * np.exp(log_w)
+    LJi, LJj = L[:, :, None] * Ji, L[:, :, None] * Jj
+    UL = np.einsum("eki,ekj->eij", Ji, LJi)
+    UR = np.einsum("eki,ekj->eij", Ji, LJj)
+    BL = np.einsum("eki,ekj->eij", Jj, LJi)
+    BR = np.einsum("eki,ekj->eij", Jj, LJj)
+    if exact:
+        a0, a1 = L[:, 0] * e[:, 0], L[:, 1] * e[:, 1]
+        htt = a0 * (-c * dx - s * dy) + a1 * (s * dx - c * dy)
+        htx = a0 * s + a1 * c
+        hty = a1 * s - a0 * c
+        UL[:, 2, 2] += htt
+        UL[:, 2, 0] += htx; UL[:, 0, 2] += htx
+        UL[:, 2, 1] += hty; UL[:, 1, 2] += hty
+        UR[:, 2, 0] -= htx; UR[:, 2, 1] -= hty
+        BL[:, 0, 2] -= htx; BL[:, 1, 2] -= hty
+    rr, cc = np.meshgrid(np.arange(3), np.arange(3), indexing="ij")
+    rows, cols, vals = [], [], []
+    for (a, b, blk) in ((ei, ei, UL), (ei, ej, UR), (ej, ei, BL), (ej, ej, BR)):
+        rows.append((3 * a[:, None, None] + rr).ravel())
+        cols.append((3 * b[:, None, None] + cc).ravel())
+        vals.append(blk.ravel())
+    rows.append(np.arange(3)); cols.append(np.arange(3)); vals.append(np.full(3, float(anchor)))
+    H = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(3 * n, 3 * n)).tocsc()
+    Le = L * e
+    xi = np.zeros(3 * n)
+    np.add.at(xi.reshape(n, 3), ei, -np.einsum("eki,ek->ei", Ji, Le))
+    np.add.at(xi.reshape(n, 3), ej, -np.einsum("eki,ek->ei", Jj, Le))
+    return H, xi
+
+
+def gn_solve_sparse(poses0, ei, ej, meas, log_w, lam, anchor=1e6, rounds=50, tol=1e-13, min_rounds=1):
+    """Gauss-Newton to convergence with sparse LU solves (update RMS below tol, after at
+    least min_rounds rounds)."""
+    import scipy.sparse.linalg as spl
+    p = np.array(poses0, np.float64, copy=True)
+    for r in range(rounds):
+        H, xi = system_sparse(p, ei, ej, meas, log_w, lam, anchor)
+        dx = spl.spsolve(H, xi, permc_spec="COLAMD").reshape(-1, 3)
+        p = p + dx
+        p[:, 2] = wrap(p[:, 2])
+        if np.sqrt(np.mean(dx ** 2)) < tol and r + 1 >= min_rounds:
+            break
+    return p
+
+
+def adjoint_sparse(poses, ei, ej, meas, log_w, lam, dL_dx, anchor=1e6):
+    """adjoint() with a sparse LU solve of the exact Hessian."""
+    import scipy.sparse.linalg as spl
+    H, _ = system_sparse(poses, ei, ej, meas, log_w, lam, anchor, exact=True)
+    mu = spl.spsolve(H, np.asarray(dL_dx, np.float64).reshape(-1), permc_spec="COLAMD").reshape(-1, 3)
+    e, Ji, Jj, _ = residuals(poses, ei, ej, meas)
+    jm = np.einsum("ekc,ec->ek", Ji, mu[ei]) + np.einsum("ekc,ec->ek", Jj, mu[ej])
+    dlw = -(lam * np.exp(log_w)) * e * jm
+    return dlw.sum() / lam, dlw, mu
+
+
+def rhs(poses, ei, ej, meas, log_w, lam):
+    """xi = -sum J^T Lambda e alone (system() without the matrix)."""
+    n = poses.shape[0]
+    e, Ji, Jj, _ = residuals(poses, ei, ej, meas)
+    Le = lam * np.exp(log_w) * e
+    xi = np.zeros(3 * n)
+    np.add.at(xi.reshape(n, 3), ei, -np.einsum("eki,ek->ei", Ji, Le))
+    np.add.at(xi.reshape(n, 3), ej, -np.einsum("eki,ek->ei", Jj, Le))
+    return xi
+
+
+def chord_solve_sparse(poses0, ei, ej, meas, log_w, lam, lu, anchor=1e6, rounds=60, tol=1e-14, min_rounds=1):
+    """Gauss-Newton's fixed point by chord iterations: every round solves with one
+    factorisation `lu` (splu of a nearby Omega, e.g. the one at the unperturbed fixed
+    point) instead of refactorising. The iteration stops where xi = 0 for THESE weights,
+    the same point Gauss-Newton reaches; it only converges more slowly. Used for the
+    finite differences, which restart from a fixed point a perturbation h away."""
+    p = np.array(poses0, np.float64, copy=True)
+    for r in range(rounds):
+        dx = lu.solve(rhs(p, ei, ej, meas, log_w, lam)).reshape(-1, 3)
+        p = p + dx
+        p[:, 2] = wrap(p[:, 2])
+        if np.sqrt(np.mean(dx ** 2)) < tol and r + 1 >= min_rounds:
+            break
+    return p

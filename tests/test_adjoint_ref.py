@@ -54,3 +54,31 @@ def test_exact_hessian_is_the_jacobian_of_the_gradient():
         x2 = R.system(p2, g.edge_i, g.edge_j, g.meas, g.log_w, lam, 0.0)[1]
         num = -(x1 - x2) / (2 * h)
         assert np.allclose(num, H[:, col], rtol=1e-5, atol=1e-5 * np.abs(H[:, col]).max())
+
+
+def test_sparse_reference_matches_dense():
+    """The sparse (SuperLU) forms of the reference equal the dense ones on a small graph:
+    Omega, the exact Hessian, the converged poses, the adjoint gradient, and the chord
+    iteration's fixed point."""
+    import scipy.sparse.linalg as spl
+    G = importlib.import_module("g-slam_on_gpu_and_fpga_b200")
+    cg = G.synth.city_grid(120, seed=2, block=5, k_closures=4, radius=3.0)
+    for exact in (False, True):
+        Hd, xd = R.system(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1, 1e12, exact=exact)
+        Hs, xs = R.system_sparse(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1, 1e12, exact=exact)
+        assert np.allclose(Hs.toarray(), Hd, rtol=0, atol=1e-9 * np.abs(Hd).max())
+        assert np.array_equal(xs, xd)
+        assert np.array_equal(R.rhs(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1), xd)
+    pd = R.gn_solve(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1, anchor=1e12)
+    ps = R.gn_solve_sparse(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1, anchor=1e12)
+    assert np.abs(ps - pd).max() <= 1e-9
+    _, dL = R.position_loss(pd, cg.gt)
+    _, gd, _ = R.adjoint(pd, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1, dL, anchor=1e12)
+    _, gs, _ = R.adjoint_sparse(pd, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1, dL, anchor=1e12)
+    assert np.linalg.norm(gs - gd) <= 1e-9 * np.linalg.norm(gd)
+    H, _ = R.system_sparse(pd, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1, 1e12)
+    lw = cg.log_w.copy()
+    lw[5, 1] += 1e-3
+    pc = R.chord_solve_sparse(pd, cg.edge_i, cg.edge_j, cg.meas, lw, 0.1, spl.splu(H.tocsc()), anchor=1e12)
+    pg = R.gn_solve_sparse(pd, cg.edge_i, cg.edge_j, cg.meas, lw, 0.1, anchor=1e12)
+    assert np.abs(pc - pg).max() <= 1e-9

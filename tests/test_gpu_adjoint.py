@@ -114,3 +114,55 @@ def test_adjoint_rejects_reference_factor_graphs(pkg):
     with pytest.raises(pkg.abi.GslamError):
         g.adjoint(np.zeros((g.n_poses, 3)))
     g.close()
+
+
+def test_adjoint_n10k_finite_differences(pkg):
+    """The adjoint at N = 10,000 (lambda 0.1, pose-0 anchor 1e12): gslam_adjoint at the
+    converged poses against (1) the exact-Hessian reference solved by sparse LU
+    (tests/adjoint_ref.py) and (2) central finite differences on 32 seeded (edge,
+    component) pairs, each difference from fixed points found by chord iterations (one
+    LU factorisation, xi = 0 for the perturbed weights) restarted at the unperturbed one.
+
+    The finite differences have an FP64 noise floor: the fixed point itself is known only
+    to the precision of xi's evaluation, so each difference carries noise ~c / (2 h).
+    Measured here against the sparse reference, relative error of the 32 differences:
+    h = 1e-3: ~2e-6 (truncation O(h^2) and noise meet); 1e-4: ~2e-5; 1e-6: ~2e-3 (noise,
+    growing as 1/h). So h = 1e-3 is the smallest step at which the 1e-5 bar holds, and
+    h = 1e-6 is checked against that measured floor, 5e-3."""
+    import scipy.sparse.linalg as spl
+    synth = importlib.import_module("g-slam_on_gpu_and_fpga_b200.synth")
+    cg = synth.city_grid(10000, seed=2)
+    p = R.gn_solve_sparse(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAM, anchor=ANCHOR, rounds=60,
+                          tol=1e-13)
+    _, dL = R.position_loss(p, cg.gt)
+    rlam, rdlw, _ = R.adjoint_sparse(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAM, dL, anchor=ANCHOR)
+    with pkg.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=LAM, anchor=ANCHOR,
+                                tol=1e-12, max_iter=400000, angle_wrap=1) as g:
+        g.poses = p
+        dlam, dlw, _, st = g.adjoint(dL)
+    gpu_vs_ref = np.linalg.norm(dlw - rdlw) / np.linalg.norm(rdlw)
+    H, _ = R.system_sparse(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAM, ANCHOR)
+    lu = spl.splu(H.tocsc(), permc_spec="COLAMD")
+    rng = np.random.default_rng(7)
+    pairs = [(int(rng.integers(len(cg.edge_i))), int(rng.integers(3))) for _ in range(32)]
+    errs = {}
+    for h in (1e-3, 1e-6):
+        fd = []
+        for e, k in pairs:
+            lw1, lw2 = cg.log_w.copy(), cg.log_w.copy()
+            lw1[e, k] += h
+            lw2[e, k] -= h
+            lp = R.position_loss(R.chord_solve_sparse(p, cg.edge_i, cg.edge_j, cg.meas, lw1, LAM, lu,
+                                                      anchor=ANCHOR, min_rounds=4), cg.gt)[0]
+            lm = R.position_loss(R.chord_solve_sparse(p, cg.edge_i, cg.edge_j, cg.meas, lw2, LAM, lu,
+                                                      anchor=ANCHOR, min_rounds=4), cg.gt)[0]
+            fd.append((lp - lm) / (2 * h))
+        fd = np.array(fd)
+        adj = np.array([dlw[e, k] for e, k in pairs])
+        errs[h] = np.linalg.norm(fd - adj) / np.linalg.norm(adj)
+    print(f"adjoint N=10000: PCG {st.iterations} iterations, residual {st.rel_residual:.1e}; "
+          f"GPU vs sparse reference {gpu_vs_ref:.2e}; vs FD h=1e-3 {errs[1e-3]:.2e}, h=1e-6 {errs[1e-6]:.2e}")
+    assert gpu_vs_ref <= 1e-6
+    assert abs(dlam - rlam) <= 1e-6 * np.abs(rdlw).sum() / LAM
+    assert errs[1e-3] <= 1e-5
+    assert errs[1e-6] <= 5e-3
