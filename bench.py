@@ -774,6 +774,17 @@ def run_ncu_case(args):
         g.close()
         torch.cuda.synchronize()
         return
+    if args.ncu_case == "batch":
+        # the 64-graph batch, 20 iterations of each solver (tol 0): one launch per solver
+        graphs, lams = c4_batch_graphs()
+        for prec in (G.abi.PREC_FP64, G.abi.PREC_MIXED):
+            b = G.PoseGraphBatch.from_se2_list(graphs, lams, precision=prec, tol=0.0, max_iter=20,
+                                               inner_max_iter=20, max_refine=1, angle_wrap=1)
+            st = b.round_all()
+            print(f"batch prec {prec}: {st[0].iterations} iterations, {st[0].solve_ms:.3f} ms", flush=True)
+            b.close()
+        g.close()
+        return
     if args.ncu_case == "spmv":
         # two launches (warm-up + one timed) of 16 FP64 copies of the matrix
         ms = g.spmv_bench(False, reps=1, n_copies=16)
@@ -800,7 +811,7 @@ def main():
                     help="skip the converged block and the N = 10k / 50k scale sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the reference GPU program comparison and the dense Gauss-Jordan sample")
-    ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv", "kernels"], default=None,
+    ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv", "kernels", "batch"], default=None,
                     help="run only two short solves of the workload (for ncu captures)")
     args = ap.parse_args()
     if args.ncu_case:

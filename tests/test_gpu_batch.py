@@ -109,3 +109,32 @@ def test_mixed_batch_converged_matches_fp64(pkg, graphs):
     for q, cg in enumerate(graphs):
         d = np.linalg.norm(poses[1][q] - poses[0][q]) / np.linalg.norm(poses[0][q] - cg.init)
         assert d <= 1e-5, (q, d)
+
+
+def test_batch_matches_oracle_per_graph(pkg, graphs, oracle):
+    """Every graph of the batch against the oracle's own round of that graph (the
+    reference's PCG restated in C, tol 1e-9): Omega and xi of the batch's linearisation
+    are the graph's own, and each graph's step dx is as close to the exact solution of
+    its system (energy norm) as the oracle's converged PCG, in FP64 and in the mixed
+    batch."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    for prec in (0, 1):
+        b = pkg.PoseGraphBatch.from_se2_list(graphs, LAMS, tol=1e-9, max_iter=200000, angle_wrap=1,
+                                             precision=prec, max_refine=500)
+        stats = b.round_all()
+        poses = b.poses
+        b.close()
+        for q, cg in enumerate(graphs):
+            blocks, _ = oracle.se2_linearise(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAMS[q])
+            dim = 3 * cg.n_poses
+            rp, ci, va, xi = oracle.csr_build_anchor(dim, cg.edge_i, cg.edge_j, blocks, 1e6)
+            x_or, _, _ = oracle.pcg(rp, ci, va, xi, tol=1e-9, max_iter=400000)
+            dx = (b.graph_poses(q, poses) - cg.init).reshape(-1)
+            dx[2::3] = (dx[2::3] + np.pi) % (2 * np.pi) - np.pi
+            A = sp.csr_matrix((va, ci, rp), shape=(dim, dim))
+            xs = spl.spsolve(A.tocsc(), xi)
+            ea = lambda x: np.sqrt(max((x - xs) @ (A @ (x - xs)), 0.0))  # noqa: E731
+            scale = np.sqrt(xs @ (A @ xs))
+            assert stats[q].rel_residual < 1e-9, (prec, q)
+            assert ea(dx) <= max(1e-6 * scale, 3.0 * ea(x_or)), (prec, q, ea(dx) / scale, ea(x_or) / scale)
