@@ -774,6 +774,16 @@ def run_ncu_case(args):
         g.close()
         torch.cuda.synchronize()
         return
+    if args.ncu_case == "gj":
+        # two dense inverses at n = 2400 (the N = 800 system's size)
+        import numpy as np
+        rng = np.random.default_rng(0)
+        a = rng.standard_normal((2400, 2400)) / np.sqrt(2400) + 4.0 * np.eye(2400)
+        for _ in range(2):
+            _, ms = G.dense.gj_inverse(a)
+            print(f"gj n=2400: {ms:.3f} ms", flush=True)
+        g.close()
+        return
     if args.ncu_case == "batch":
         # the 64-graph batch, 20 iterations of each solver (tol 0): one launch per solver
         graphs, lams = c4_batch_graphs()
@@ -811,7 +821,7 @@ def main():
                     help="skip the converged block and the N = 10k / 50k scale sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the reference GPU program comparison and the dense Gauss-Jordan sample")
-    ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv", "kernels", "batch"], default=None,
+    ap.add_argument("--ncu-case", choices=["fp64", "mixed", "spmv", "kernels", "batch", "gj"], default=None,
                     help="run only two short solves of the workload (for ncu captures)")
     args = ap.parse_args()
     if args.ncu_case:
