@@ -77,54 +77,63 @@ __global__ void k_gj_copy_col(int n, const double *__restrict__ A, int k0, doubl
 }
 
 /*
- * P = inv(U[K, :]) by in-place Gauss-Jordan without pivoting, one CTA of 256 threads
- * with the 64 x 64 block in registers: thread t owns row r = t / 4 and columns
- * [16 g, 16 g + 16), g = t % 4, so a warp holds 8 whole rows. Pivot step i: every
- * thread takes f = T[r][i] from the lane of its row that owns column i (a shuffle inside
- * the row's four lanes); the four threads of row i form the new pivot row
- * (T[i][i] -> 1, then every entry times p = 1 / T[i][i]) and write it to one of two
- * shared buffers; one CTA barrier; every other row does T[r][c] -= f * pivot[c] with
- * T[r][i] -> 0 first. Per element the same operations as the unblocked elimination
- * (src/cpu_pcg_fp64/MatrixOps.c:29-91: the ratio, then the subtraction). The two
- * buffers alternate, so one barrier per step suffices: the buffer written at step i was
- * last read at step i - 2, before every thread passed step i - 1's barrier.
+ * In-place Gauss-Jordan inverse (no pivoting) of a 64 x 64 block held in registers by the
+ * NT threads of a CTA: thread t owns row r = t / (NT / 64) and the W = 64 / (NT / 64)
+ * columns [W g, W g + W), g = t % (NT / 64), so a warp holds whole rows. Pivot step i:
+ * every thread takes f = T[r][i] from the lane of its row that owns column i (a shuffle
+ * inside the row's lanes); the threads of row i form the new pivot row (T[i][i] -> 1,
+ * then every entry times p = 1 / T[i][i]) and write it to one of two shared buffers; one
+ * CTA barrier; every other row does T[r][c] -= f * pivot[c] with T[r][i] -> 0 first. Per
+ * element the same operations as the unblocked elimination
+ * (src/cpu_pcg_fp64/MatrixOps.c:29-91: the ratio, then the subtraction). The two buffers
+ * alternate, so one barrier per step suffices: the buffer written at step i was last
+ * read at step i - 2, before every thread passed step i - 1's barrier.
  */
-__global__ void __launch_bounds__(256) k_gj_diag(const double *__restrict__ U, int k0, double *__restrict__ P) {
-    __shared__ __align__(16) double s_prow[2][GJ_B];
-    const int t = threadIdx.x, r = t >> 2, g = t & 3;
-    const int row_lane0 = (t & 31) & ~3; /* this row's first lane in the warp */
-    double T[16];
-    const double *src = U + (size_t)(k0 + r) * GJ_B + 16 * g;
+template <int NT>
+__device__ __forceinline__ void invert64_regs(double (&T)[64 / (NT / 64)], double (*s_prow)[GJ_B]) {
+    constexpr int LPR = NT / 64, W = 64 / LPR; /* lanes per row, columns per lane */
+    const int t = threadIdx.x, r = t / LPR, g = t % LPR;
+    const int row_lane0 = (t & 31) - g; /* this row's first lane in the warp */
+    for (int gi = 0; gi < LPR; gi++) {
 #pragma unroll
-    for (int j = 0; j < 16; j++) T[j] = src[j];
-    for (int gi = 0; gi < 4; gi++) {
-#pragma unroll
-        for (int jj = 0; jj < 16; jj++) {
-            const int i = 16 * gi + jj, buf = i & 1;
+        for (int jj = 0; jj < W; jj++) {
+            const int i = W * gi + jj, buf = i & 1;
             const double f = __shfl_sync(0xffffffffu, T[jj], row_lane0 + gi);
             if (r == i) {
                 const double p = 1.0 / f;
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const double v = (16 * g + j == i) ? 1.0 : T[j];
+                for (int j = 0; j < W; j++) {
+                    const double v = (W * g + j == i) ? 1.0 : T[j];
                     T[j] = v * p;
-                    s_prow[buf][16 * g + j] = T[j];
+                    s_prow[buf][W * g + j] = T[j];
                 }
             }
             __syncthreads();
             if (r != i) {
-                const double2 *pr = reinterpret_cast<const double2 *>(&s_prow[buf][16 * g]);
+                const double2 *pr = reinterpret_cast<const double2 *>(&s_prow[buf][W * g]);
 #pragma unroll
-                for (int j = 0; j < 16; j += 2) {
+                for (int j = 0; j < W; j += 2) {
                     const double2 q = pr[j >> 1];
-                    const double v0 = (16 * g + j == i) ? 0.0 : T[j];
-                    const double v1 = (16 * g + j + 1 == i) ? 0.0 : T[j + 1];
+                    const double v0 = (W * g + j == i) ? 0.0 : T[j];
+                    const double v1 = (W * g + j + 1 == i) ? 0.0 : T[j + 1];
                     T[j] = v0 - f * q.x;
                     T[j + 1] = v1 - f * q.y;
                 }
             }
         }
     }
+}
+
+/* P = inv(U[K, :]): the first step's pivot block (later ones are inverted by the update
+ * tile that produces them, k_gj_update) */
+__global__ void __launch_bounds__(256) k_gj_diag(const double *__restrict__ U, int k0, double *__restrict__ P) {
+    __shared__ __align__(16) double s_prow[2][GJ_B];
+    const int t = threadIdx.x, r = t >> 2, g = t & 3;
+    double T[16];
+    const double *src = U + (size_t)(k0 + r) * GJ_B + 16 * g;
+#pragma unroll
+    for (int j = 0; j < 16; j++) T[j] = src[j];
+    invert64_regs<256>(T, s_prow);
     double *dst = P + (size_t)r * GJ_B + 16 * g;
 #pragma unroll
     for (int j = 0; j < 16; j++) dst[j] = T[j];
@@ -162,13 +171,17 @@ __global__ void __launch_bounds__(128) k_gj_row_panel(int n, double *__restrict_
 /* trailing update and column panel, one CTA per 64x64 tile (I, J), I != K:
  *   J != K: A[I, J] -= U[I] A[K, J];   J == K: A[I, K] = -U[I] P.
  * Tile (K, K) writes P. The old A[I, J] is loaded into registers before the operand tiles
- * (its latency overlaps theirs); tiles of the next pivot column also go to Un. */
+ * (its latency overlaps theirs); tiles of the next pivot column also go to Un. Tiles are
+ * numbered from the next pivot tile (K + 1, K + 1), so that tile is the first block
+ * scheduled: it goes on to invert itself into Pn, the next step's pivot inverse, while
+ * the other tiles are updated (the inversion is off the step's critical path). */
 __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A, int k0,
                                                    const double *__restrict__ U, const double *__restrict__ P,
-                                                   double *__restrict__ Un) {
+                                                   double *__restrict__ Un, double *__restrict__ Pn) {
     extern __shared__ __align__(16) double sm[];
     double *sA = sm, *sB = sm + GJ_B * GJ_LD;
-    const int ti = blockIdx.y, tj = blockIdx.x;
+    const int nt = n / GJ_B, kn = k0 / GJ_B + 1;
+    const int ti = ((int)blockIdx.y + kn) % nt, tj = ((int)blockIdx.x + kn) % nt;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wm = warp >> 1, wn = warp & 1;
     const int gid = lane >> 2, tig = lane & 3;
     if (64 * ti == k0) {
@@ -178,6 +191,7 @@ __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A
         return;
     }
     const bool colp = (64 * tj == k0), next = (64 * tj == k0 + GJ_B);
+    const bool pivot_next = next && ti == kn;
     double old[4][4][2];
     if (!colp) {
 #pragma unroll
@@ -195,6 +209,7 @@ __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A
     __syncthreads();
     double acc[4][4][2] = {};
     tile_mma(sA, sB, wm, wn, lane, acc);
+    if (pivot_next) __syncthreads(); /* sA is reused below */
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -205,7 +220,21 @@ __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A
             else v = make_double2(old[i][j][0] - acc[i][j][0], old[i][j][1] - acc[i][j][1]);
             *reinterpret_cast<double2 *>(A + (size_t)(64 * ti + r) * n + 64 * tj + c) = v;
             if (next) *reinterpret_cast<double2 *>(Un + (size_t)(64 * ti + r) * GJ_B + c) = v;
+            if (pivot_next) *reinterpret_cast<double2 *>(sA + r * GJ_LD + c) = v;
         }
+    if (pivot_next) {
+        /* the next pivot block, row-owned (thread t: row t / 2, 32 columns), inverted in place */
+        __shared__ __align__(16) double s_prow[2][GJ_B];
+        __syncthreads();
+        const int t = threadIdx.x, r = t >> 1, g = t & 1;
+        double T[32];
+#pragma unroll
+        for (int j = 0; j < 32; j++) T[j] = sA[r * GJ_LD + 32 * g + j];
+        invert64_regs<128>(T, s_prow);
+#pragma unroll
+        for (int j = 0; j < 32; j += 2)
+            *reinterpret_cast<double2 *>(Pn + (size_t)r * GJ_B + 32 * g + j) = make_double2(T[j], T[j + 1]);
+    }
 }
 
 /* pad: B (m x m, m = n rounded up to 64) = diag(A, I) */
@@ -236,10 +265,10 @@ __global__ void k_gemv(int m, const double *__restrict__ A, const double *__rest
 
 static int gj_run(int m, double *d_a, cudaStream_t st, double *scratch) {
     /* scratch: two copies of a block column (m x 64 each, this step's and the next's) then
-     * P (64 x 64); the first step's copy is made here, every later one by the previous
-     * step's row panel and trailing update */
+     * two pivot inverses (64 x 64 each); the first step's copy and inverse are made here,
+     * every later one by the previous step's row panel and trailing update */
     double *Ub[2] = { scratch, scratch + (size_t)m * GJ_B };
-    double *P = scratch + 2 * (size_t)m * GJ_B;
+    double *Pb[2] = { scratch + 2 * (size_t)m * GJ_B, scratch + 2 * (size_t)m * GJ_B + GJ_B * GJ_B };
     const size_t smem = 2 * GJ_B * GJ_LD * sizeof(double);
     static bool attr = false;
     if (!attr) {
@@ -249,12 +278,13 @@ static int gj_run(int m, double *d_a, cudaStream_t st, double *scratch) {
     }
     const int nt = m / GJ_B;
     k_gj_copy_col<<<(m * GJ_B + 255) / 256, 256, 0, st>>>(m, d_a, 0, Ub[0]);
+    k_gj_diag<<<1, 256, 0, st>>>(Ub[0], 0, Pb[0]);
     for (int k = 0; k < nt; k++) {
         const int k0 = GJ_B * k;
         double *U = Ub[k & 1], *Un = Ub[(k + 1) & 1];
-        k_gj_diag<<<1, 256, 0, st>>>(U, k0, P);
+        double *P = Pb[k & 1], *Pn = Pb[(k + 1) & 1];
         k_gj_row_panel<<<nt, 128, smem, st>>>(m, d_a, k0, P, Un);
-        k_gj_update<<<dim3(nt, nt), 128, smem, st>>>(m, d_a, k0, U, P, Un);
+        k_gj_update<<<dim3(nt, nt), 128, smem, st>>>(m, d_a, k0, U, P, Un, Pn);
     }
     return cudaGetLastError() == cudaSuccess ? GSLAM_OK : GSLAM_ERR_CUDA;
 }
@@ -267,7 +297,7 @@ int gslam_gj_inverse(int n, double *d_a, int lda, void *stream, float *ms) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int rc = GSLAM_ERR_CUDA;
     if (cudaMalloc(&B, (size_t)m * m * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&scratch, (2 * (size_t)m * GJ_B + GJ_B * GJ_B) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&scratch, (2 * (size_t)m * GJ_B + 2 * GJ_B * GJ_B) * sizeof(double)) != cudaSuccess ||
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         gslam_set_last_error("cudaMalloc failed (dense inverse)");
         goto done;
