@@ -136,8 +136,11 @@ template <> struct BVec<float> {
         z(P.zf4), pa(P.pfa4), pb(P.pfb4), q(P.qf4) {}
 };
 
+/* launch bound of two CTAs per SM: 512-thread CTAs fit in 64 registers without spills, so
+ * the tuner's ctas_per_sm = 2 gives 32 warps per SM to hide the gathers' latency (one CTA
+ * of 128-register threads left the kernel waiting on memory with 16 warps per SM) */
 template <int BS, typename T>
-__global__ void __launch_bounds__(BS, 1) k_pcg_batch(PcgParams P, BatchParams B) {
+__global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B) {
     const BVec<T> V(P, B);
     extern __shared__ __align__(16) double s_part[]; /* [slices of this CTA][2] */
     __shared__ double s_rz[BATCH_LG_MAX], s_rr[BATCH_LG_MAX], s_bn[BATCH_LG_MAX];
