@@ -249,34 +249,6 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 L->smem_val_cap = std::min<int64_t>(cap64, 9 * max_slots);
                 L->smem_p_off = 8 * L->smem_val_cap + col_bytes;
                 L->smem_bytes = (size_t)(L->smem_p_off + p_bytes);
-                /* which block positions of each slice are staged: with C positions of room
-                 * for a CTA, every slice keeps its first T positions, T the largest with
-                 * sum_s min(L_s, T) <= C (all of them when the share fits) */
-                const int64_t cap_pos = L->smem_val_cap / 288;
-                std::vector<int> sm_pos(std::max(S.n_slices, 1), 0), sm_len(std::max(S.n_slices, 1), 0);
-                for (int i = 0; i < rgrid; i++) {
-                    auto positions = [&](int sl) { return (int)((S.slice_ptr[sl + 1] - S.slice_ptr[sl]) / 32); };
-                    auto used = [&](int t) {
-                        int64_t u = 0;
-                        for (int sl = cs[i]; sl < cs[i + 1]; sl++) u += std::min(positions(sl), t);
-                        return u;
-                    };
-                    int lo = 0, hi = 0;
-                    for (int sl = cs[i]; sl < cs[i + 1]; sl++) hi = std::max(hi, positions(sl));
-                    while (lo < hi) { /* largest T with used(T) <= cap_pos */
-                        const int mid = lo + (hi - lo + 1) / 2;
-                        if (used(mid) <= cap_pos) lo = mid;
-                        else hi = mid - 1;
-                    }
-                    int pos = 0;
-                    for (int sl = cs[i]; sl < cs[i + 1]; sl++) {
-                        sm_pos[sl] = pos;
-                        sm_len[sl] = std::min(positions(sl), lo);
-                        pos += sm_len[sl];
-                    }
-                }
-                CK(dupload(m, st, &L->res_sm_pos, sm_pos));
-                CK(dupload(m, st, &L->res_sm_len, sm_len));
             }
             /* mixed: FP32 values | local columns | D^-1 of own rows (2304 B per slice) |
              * z of own and halo rows (16 B each) | u, v of the first `block` halo rows
@@ -399,8 +371,6 @@ static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts 
     P.halo_rows = L->halo_rows;
     P.row_export = L->row_export;
     P.smem_p_off = L->smem_p_off;
-    P.res_sm_pos = L->res_sm_pos;
-    P.res_sm_len = L->res_sm_len;
     tr.step("memsets");
     CK(record_event(L->ev0, st));
     if (mixed) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->mixed_smem_bytes));

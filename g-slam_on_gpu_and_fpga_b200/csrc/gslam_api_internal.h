@@ -46,7 +46,6 @@ struct DevLayout {
     int *lcol = nullptr, *halo_ptr = nullptr, *halo_rows = nullptr; /* CTA-local columns, halo lists */
     unsigned char *row_export = nullptr; /* rows some other CTA's halo lists */
     int64_t smem_p_off = 0;        /* staged p, after values and columns */
-    int *res_sm_pos = nullptr, *res_sm_len = nullptr; /* per slice: staged block positions (FP64 values) */
     size_t smem_bytes = 0;
     bool mixed_ok = false;          /* the mixed solver's shared-memory layout fits */
     int64_t mixed_val_cap = 0;     /* floats staged per CTA */

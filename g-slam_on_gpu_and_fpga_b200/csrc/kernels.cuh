@@ -86,8 +86,6 @@ struct PcgParams {
     const int *halo_rows;  /* resident solver: halo rows (new row indices) */
     const unsigned char *row_export; /* 1 for rows in another CTA's halo: only those are published */
     int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
-    const int *res_sm_pos; /* resident solver, per slice: first shared-memory block position of its values */
-    const int *res_sm_len; /* resident solver, per slice: leading block positions staged (the rest from L2) */
 };
 
 /* Round cost terms per edge and their total (kernels.cu); block_sums holds

@@ -9,11 +9,7 @@
  * the sliced matrix into shared memory once, with one TMA bulk copy
  * (cp.async.bulk, completion on an mbarrier), and every PCG iteration after that
  * reads values and column indices from shared memory. A share that does not fit
- * keeps the same number of leading block positions of every slice in shared memory
- * (the largest T with sum over its slices of min(positions, T) within the capacity,
- * chosen on the host) and reads each slice's positions beyond T from global memory
- * (L2): every warp then has a short tail instead of a few warps reading whole slices
- * from L2 while the rest wait for them.
+ * reads its tail blocks from global memory (L2) instead.
  *
  * Each thread owns one block row for the whole solve and keeps that row's x, r,
  * z and p in registers. Only what other CTAs need crosses L2 each iteration: p
@@ -58,6 +54,8 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
 
     const int s0 = __ldg(P.cta_slice + blockIdx.x), s1 = __ldg(P.cta_slice + blockIdx.x + 1);
     const int64_t slot0 = __ldg(P.slice_ptr + s0), slot1 = __ldg(P.slice_ptr + s1);
+    const int64_t nval = 9 * (slot1 - slot0);
+    const int64_t nsm = nval < P.smem_val_cap ? nval : P.smem_val_cap; /* multiple of 288 */
     double *sval = reinterpret_cast<double *>(smem);
     int *scol = reinterpret_cast<int *>(smem + 8 * P.smem_val_cap);   /* local column indices */
     double *sp = reinterpret_cast<double *>(smem + P.smem_p_off);     /* p of own + halo rows */
@@ -71,17 +69,9 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        /* each slice's first sm_len block positions (288 values each) go to shared memory at
-         * position sm_pos; the rest of the slice stays in global memory */
-        unsigned vbytes = 0;
-        for (int sl = s0; sl < s1; sl++) vbytes += 2304u * (unsigned)__ldg(P.res_sm_len + sl);
-        const unsigned cbytes = (unsigned)(4 * (slot1 - slot0));
+        const unsigned vbytes = (unsigned)(8 * nsm), cbytes = (unsigned)(4 * (slot1 - slot0));
         tma_mbar_expect_tx(&s_bar, vbytes + cbytes);
-        for (int sl = s0; sl < s1; sl++) {
-            const unsigned b = 2304u * (unsigned)__ldg(P.res_sm_len + sl);
-            if (b) tma_bulk_g2s(sval + 288 * (size_t)__ldg(P.res_sm_pos + sl), P.val + 9 * __ldg(P.slice_ptr + sl), b,
-                                &s_bar);
-        }
+        if (vbytes) tma_bulk_g2s(sval, P.val + 9 * slot0, vbytes, &s_bar);
         if (cbytes) tma_bulk_g2s(scol, P.lcol + slot0, cbytes, &s_bar);
         int ok = tma_wait(&s_bar, 0, P.spin_limit);
         if (!ok) {
@@ -105,8 +95,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     const int len = mine ? __ldg(P.row_len + row) : 0;
     const int lslot = own_slice ? (int)(__ldg(P.slice_ptr + s) - slot0) : 0; /* local slot of (j=0) */
     /* how many of the row's blocks have their values in shared memory */
-    const int j_sm = own_slice ? min(len, __ldg(P.res_sm_len + s)) : 0;
-    const double *sv_row = sval + 288 * (own_slice ? __ldg(P.res_sm_pos + s) : 0) + lane;
+    const int j_sm = min(len, max(0, ((int)nsm - 9 * lslot) / 288));
     const double *gval = P.val + 9 * slot0;  /* global copy of this CTA's share */
     const int *cb = scol + lslot + lane;
 
@@ -162,7 +151,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
             /* blocks with values in shared memory, four at a time (their column and p
              * loads in flight together), then the share's tail from L2, two at a time;
              * a row's blocks are added in ascending column order either way */
-            const double *sv0 = sv_row;
+            const double *sv0 = sval + 9 * lslot + lane;
             int j = 0;
             for (; j + 3 < j_sm; j += 4) {
                 const int c0 = cb[32 * j], c1 = cb[32 * (j + 1)], c2 = cb[32 * (j + 2)], c3 = cb[32 * (j + 3)];
