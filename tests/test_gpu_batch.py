@@ -137,4 +137,11 @@ def test_batch_matches_oracle_per_graph(pkg, graphs, oracle):
             ea = lambda x: np.sqrt(max((x - xs) @ (A @ (x - xs)), 0.0))  # noqa: E731
             scale = np.sqrt(xs @ (A @ xs))
             assert stats[q].rel_residual < 1e-9, (prec, q)
+            if scale < 1e-9:
+                # nothing to solve (a walk without closures: the guess is already optimal);
+                # the step is rounding noise, so compare the poses at rounding level
+                p_or = cg.init + x_or.reshape(-1, 3)
+                p_or[:, 2] = (p_or[:, 2] + np.pi) % (2 * np.pi) - np.pi
+                assert np.abs(b.graph_poses(q, poses) - p_or).max() <= 1e-12 * max(1.0, np.abs(p_or).max())
+                continue
             assert ea(dx) <= max(1e-6 * scale, 3.0 * ea(x_or)), (prec, q, ea(dx) / scale, ea(x_or) / scale)
