@@ -61,11 +61,20 @@ __device__ __forceinline__ void tile_mma(const double *sA, const double *sB, int
     }
 }
 
+/* 64x64 tile g (leading dimension ld, a multiple of 2) -> shared s (ld GJ_LD): 16-byte
+ * asynchronous copies through L2 (cp.async.cg), all of a thread's in flight together;
+ * complete after load_tile_wait (then a CTA barrier before reading other threads' parts) */
 __device__ __forceinline__ void load_tile(double *s, const double *g, int ld) {
-    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) {
-        const int r = t >> 6, c = t & 63;
-        s[r * GJ_LD + c] = g[(size_t)r * ld + c];
+    for (int t = threadIdx.x; t < GJ_B * GJ_B / 2; t += blockDim.x) {
+        const int r = t >> 5, c = 2 * (t & 31);
+        const unsigned d = (unsigned)__cvta_generic_to_shared(s + r * GJ_LD + c);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g + (size_t)r * ld + c) : "memory");
     }
+}
+
+__device__ __forceinline__ void load_tile_wait() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 /* U = A[:, K] (n x 64, ld 64) */
@@ -152,6 +161,7 @@ __global__ void __launch_bounds__(128) k_gj_row_panel(int n, double *__restrict_
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wm = warp >> 1, wn = warp & 1;
     load_tile(sA, P, GJ_B);
     load_tile(sB, A + (size_t)k0 * n + 64 * tj, n);
+    load_tile_wait();
     __syncthreads();
     double acc[4][4][2] = {};
     tile_mma(sA, sB, wm, wn, lane, acc);
@@ -206,6 +216,7 @@ __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A
     }
     load_tile(sA, U + (size_t)(64 * ti) * GJ_B, GJ_B);
     load_tile(sB, colp ? P : A + (size_t)k0 * n + 64 * tj, colp ? GJ_B : n);
+    load_tile_wait();
     __syncthreads();
     double acc[4][4][2] = {};
     tile_mma(sA, sB, wm, wn, lane, acc);
