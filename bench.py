@@ -376,12 +376,14 @@ def batch_sample(G, torch, rounds, world, rank, dist):
         b = G.PoseGraphBatch.from_se2_list(mine, mlams, **opts)
         b.round_all()                                      # warm-up
         b.poses = b.init_poses
-        ms, its = 0.0, []
+        ms, its, fallbacks = 0.0, [], 0
         for _ in range(rounds):
             st = b.round_all()
             ms += st[0].round_ms
             its += [x.iterations for x in st]
-        out[name] = dict(poses=b.poses, ms=max_over_ranks(dist, ms), its=float(np.mean(its)), b=b)
+            fallbacks += sum(1 for x in st if x.refinements < 0)
+        out[name] = dict(poses=b.poses, ms=max_over_ranks(dist, ms), its=float(np.mean(its)), b=b,
+                         fallbacks=fallbacks)
     # pose error of the timed rounds against single-graph FP64 rounds (first 8 of the share)
     errs = {"fp64": [], "mixed": []}
     for q, g in enumerate(mine[:8]):
@@ -402,7 +404,8 @@ def batch_sample(G, torch, rounds, world, rank, dist):
             "unit": "graph GN iters/s (all graphs, one persistent launch per PCG pass)",
             "ms_per_round": round(out["mixed"]["ms"] / rounds, 3),
             "fp64_ms_per_round": round(out["fp64"]["ms"] / rounds, 3),
-            "pcg_iterations_mean": out["mixed"]["its"],
+            "pcg_iterations_mean": out["mixed"]["its"], "fp64_pcg_iterations_mean": out["fp64"]["its"],
+            "mixed_graph_solves_finished_in_fp64": out["mixed"]["fallbacks"],
             "tuned": best, "tuning_us_per_iteration": {str(c): (round(t, 2) if t else None) for c, t in timings},
             "max_rel_pose_err_vs_single_fp64": {k: (max(v) if v else None) for k, v in errs.items()},
             "dtype": "mixed: f32 inner / f64 refinement; fp64: f64",
