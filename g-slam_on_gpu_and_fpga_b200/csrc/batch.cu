@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B)
     for (int sl = warp; sl < ns; sl += W) {
         const int row = 32 * (s0 + sl) + lane;
         double rz = 0.0, rr = 0.0;
-        if (row < P.n_rows) {
+        const bool skipped = B.skip != nullptr && __ldg(B.skip + __ldg(B.slice_graph + s0 + sl)) != 0;
+        if (row < P.n_rows && !skipped) {
             const TV<T> b = tv_ldg(V.b, row);
             tv_st(V.x, row, TV<T>{ 0, 0, 0 });
             tv_st(V.r, row, b);

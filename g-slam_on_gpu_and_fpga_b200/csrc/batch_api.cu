@@ -206,7 +206,7 @@ int gslam_create_se2_batch(const gslam_se2_graph *graphs, uint32_t n_graphs, con
 
 static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total);
 
-int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total) {
+int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total, const int *d_skip) {
     if (g->o.precision == GSLAM_PREC_MIXED) return batch_solve_mixed(g, per_graph, total);
     BatchState &B = *g->batch;
     DevLayout *L = &g->L;
@@ -249,6 +249,7 @@ int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats 
     BP.partials = B.d_partials;
     BP.res = B.d_res;
     BP.active = B.d_active;
+    BP.skip = d_skip;
     CK(cudaMemsetAsync(L->gs, 0, sizeof(GridSync), st));
     CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
     CK(cudaMemsetAsync(B.d_res, 0, B.n_graphs * sizeof(PcgResult), st));
@@ -402,20 +403,27 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
     float solve_ms = 0.f;
     solve_ms = elapsed_ms(L->ev0, L->ev1);
     if (stagnated) {
-        /* the FP32 inner solves cannot resolve at least one graph: FP64 for the batch */
-        gslam_solve_stats s64;
+        /* the FP32 inner solves cannot resolve these graphs: solve just them again in FP64
+         * (from x = 0, the reference's start); every other graph keeps its mixed solution */
+        std::vector<int> skip(G);
+        for (int q = 0; q < G; q++) skip[q] = reason[q] == GSLAM_STOP_STAGNATION ? 0 : 1;
+        if (!B.d_skip) CK(dalloc(m, &B.d_skip, (size_t)G));
+        CK(cudaMemcpyAsync(B.d_skip, skip.data(), G * sizeof(int), cudaMemcpyHostToDevice, st));
+        std::vector<gslam_solve_stats> s64(G);
+        gslam_solve_stats tot64;
         gslam_opts keep = g->o;
         g->o.precision = GSLAM_PREC_FP64;
-        rc = batch_solve(g, per_graph, &s64);
+        rc = batch_solve(g, s64.data(), &tot64, B.d_skip);
         g->o = keep;
-        if (per_graph)
-            for (int q = 0; q < G; q++) {
-                per_graph[q].iterations += its[q];
-                per_graph[q].refinements = -refs[q];
-                per_graph[q].solve_ms += solve_ms;
+        if (rc != GSLAM_OK) return rc;
+        for (int q = 0; q < G; q++)
+            if (!skip[q]) {
+                its[q] += s64[q].iterations;
+                refs[q] = -refs[q];
+                reason[q] = s64[q].reason;
+                rel[q] = s64[q].rel_residual;
             }
-        if (total) { *total = s64; total->solve_ms += solve_ms; }
-        return rc;
+        solve_ms += (float)tot64.solve_ms;
     }
     gslam_solve_stats agg;
     memset(&agg, 0, sizeof agg);

@@ -79,6 +79,7 @@ struct BatchState {
     float *d_bf4 = nullptr;
     int *d_gactive = nullptr;
     double *d_gres = nullptr, *h_gres = nullptr;
+    int *d_skip = nullptr;       /* graphs the FP64 rerun of a stagnated mixed batch leaves alone */
     /* chunk sums of the per-graph norm kernels */
     double *d_chunk_part = nullptr;
     int max_chunks = 1;
@@ -189,6 +190,7 @@ int common_setup(gslam_graph *g, const gslam_opts *opts);
 int finish_setup(gslam_graph *g, const std::vector<unsigned> &t1, const std::vector<unsigned> &t2,
                  const std::vector<int> *diag_rows = nullptr, const std::vector<int> *segments = nullptr);
 /* the batched solve behind gslam_solve / gslam_round on a batch handle (batch_api.cu) */
-int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total);
+int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total,
+                const int *d_skip = nullptr);
 
 #endif

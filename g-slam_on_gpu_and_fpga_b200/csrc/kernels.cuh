@@ -121,6 +121,9 @@ struct BatchParams {
     PcgResult *res;          /* [n_graphs] */
     int *active;             /* graphs still iterating (set to n_graphs before launch) */
     const float *bf4;        /* FP32 inner solve: right-hand side (padded rows) */
+    const int *skip;         /* [n_graphs] or null: graphs left exactly as they are (done from the
+                              * start, their vectors untouched: the mixed batch's FP64 rerun of
+                              * only the graphs that stagnated) */
 };
 /* fp32: the inner solve of the mixed batch (FP32 values / vectors in PcgParams' FP32
  * fields, right-hand side bf4); otherwise the FP64 PCG on val / b4. */
