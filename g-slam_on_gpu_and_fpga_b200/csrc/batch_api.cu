@@ -32,7 +32,7 @@ static int batch_partition(gslam_graph *g) {
     int n_sm = 0;
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, g->device));
     B.block = g->o.threads_per_cta ? g->o.threads_per_cta : 512;
-    const int cps = g->o.ctas_per_sm ? g->o.ctas_per_sm : 1;
+    const int cps = g->o.ctas_per_sm ? g->o.ctas_per_sm : 2; /* two 64-register CTAs per SM by default */
     const int warps = B.block / 32;
     /* slices per CTA: room to balance by slot count, at least one per warp */
     int grid_guess = cps * n_sm;

@@ -7,8 +7,8 @@
  * pivoting and multiplies xi by the inverse; it is kept for small N as a check of
  * the iterative solvers. Here the same elimination (no pivoting) is blocked by
  * b = 64 columns; step k with K = [64k, 64k + 64):
- *   U = A[:, K] (copy of the old block column), P = A[K, K]^-1 (one CTA, unblocked
- *   in-place Gauss-Jordan with the block in registers),
+ *   U = A[:, K] (copy of the old block column), P = A[K, K]^-1 (one CTA: recursive
+ *   halving down to 16 x 16 Gauss-Jordan in a warp, see inv_block),
  *   A[K, J] = P A[K, J]                 for J != K   (row panel)
  *   A[I, J] = A[I, J] - U[I] A[K, J]    for I, J != K (trailing update, rank 64)
  *   A[I, K] = -U[I] P                   for I != K,   A[K, K] = P.
@@ -86,66 +86,128 @@ __global__ void k_gj_copy_col(int n, const double *__restrict__ A, int k0, doubl
 }
 
 /*
- * In-place Gauss-Jordan inverse (no pivoting) of a 64 x 64 block held in registers by the
- * NT threads of a CTA: thread t owns row r = t / (NT / 64) and the W = 64 / (NT / 64)
- * columns [W g, W g + W), g = t % (NT / 64), so a warp holds whole rows. Pivot step i:
- * every thread takes f = T[r][i] from the lane of its row that owns column i (a shuffle
- * inside the row's lanes); the threads of row i form the new pivot row (T[i][i] -> 1,
- * then every entry times p = 1 / T[i][i]) and write it to one of two shared buffers; one
- * CTA barrier; every other row does T[r][c] -= f * pivot[c] with T[r][i] -> 0 first. Per
- * element the same operations as the unblocked elimination
- * (src/cpu_pcg_fp64/MatrixOps.c:29-91: the ratio, then the subtraction). The two buffers
- * alternate, so one barrier per step suffices: the buffer written at step i was last
- * read at step i - 2, before every thread passed step i - 1's barrier.
+ * The 64 x 64 pivot-block inverse, blocked recursively so that few steps are serial (by a
+ * CTA of 128 threads, the block in shared memory). With M = [A B; C D] in halves and no
+ * pivoting (the same pivot order as Gauss-Jordan, src/cpu_pcg_fp64/MatrixOps.c:29-91):
+ *   A <- A^-1;  W = A^-1 B;  V = C A^-1;  S = D - C W;  D <- S^-1;
+ *   B <- -W S^-1;  C <- -S^-1 V;  A <- A^-1 - W C   (= A^-1 + W S^-1 V),
+ * 32 x 32 halves split the same way into 16 x 16 ones, and a 16 x 16 block is inverted by
+ * Gauss-Jordan in one warp (two lanes per row, the pivot row by warp shuffles). Serial
+ * path: four 16-pivot warp eliminations and a few small GEMMs, instead of 64 pivot steps
+ * each behind a CTA barrier.
  */
-template <int NT>
-__device__ __forceinline__ void invert64_regs(double (&T)[64 / (NT / 64)], double (*s_prow)[GJ_B]) {
-    constexpr int LPR = NT / 64, W = 64 / LPR; /* lanes per row, columns per lane */
-    const int t = threadIdx.x, r = t / LPR, g = t % LPR;
-    const int row_lane0 = (t & 31) - g; /* this row's first lane in the warp */
-    for (int gi = 0; gi < LPR; gi++) {
+
+/* Gauss-Jordan without pivoting of the 16 x 16 block at m (leading dimension ld), by the
+ * 32 lanes of one warp: lane l holds row l / 2, columns [8 (l % 2), 8 (l % 2) + 8). Pivot
+ * step i: f = T[r][i] from the lane of row r that owns column i; the two lanes of row i
+ * form the new pivot row (T[i][i] -> 1, then times 1 / T[i][i]); every lane takes the
+ * pivot row's entries of its own columns by shuffles; the other rows subtract f times
+ * them with T[r][i] -> 0 first. */
+__device__ __forceinline__ void inv16_warp(double *m, int ld) {
+    const int lane = threadIdx.x & 31, r = lane >> 1, h = lane & 1;
+    double T[8];
 #pragma unroll
-        for (int jj = 0; jj < W; jj++) {
-            const int i = W * gi + jj, buf = i & 1;
-            const double f = __shfl_sync(0xffffffffu, T[jj], row_lane0 + gi);
-            if (r == i) {
-                const double p = 1.0 / f;
+    for (int j = 0; j < 8; j++) T[j] = m[r * ld + 8 * h + j];
 #pragma unroll
-                for (int j = 0; j < W; j++) {
-                    const double v = (W * g + j == i) ? 1.0 : T[j];
-                    T[j] = v * p;
-                    s_prow[buf][W * g + j] = T[j];
-                }
-            }
-            __syncthreads();
-            if (r != i) {
-                const double2 *pr = reinterpret_cast<const double2 *>(&s_prow[buf][W * g]);
+    for (int i = 0; i < 16; i++) {
+        const int gi = i >> 3, jj = i & 7;
+        const double f = __shfl_sync(0xffffffffu, T[jj], 2 * r + gi);
+        if (r == i) {
+            const double p = 1.0 / f;
 #pragma unroll
-                for (int j = 0; j < W; j += 2) {
-                    const double2 q = pr[j >> 1];
-                    const double v0 = (W * g + j == i) ? 0.0 : T[j];
-                    const double v1 = (W * g + j + 1 == i) ? 0.0 : T[j + 1];
-                    T[j] = v0 - f * q.x;
-                    T[j + 1] = v1 - f * q.y;
-                }
-            }
+            for (int j = 0; j < 8; j++) T[j] = ((8 * h + j == i) ? 1.0 : T[j]) * p;
+        }
+        double q[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) q[j] = __shfl_sync(0xffffffffu, T[j], 2 * i + h);
+        if (r != i) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) T[j] = ((8 * h + j == i) ? 0.0 : T[j]) - f * q[j];
         }
     }
+#pragma unroll
+    for (int j = 0; j < 8; j++) m[r * ld + 8 * h + j] = T[j];
 }
 
+/* out = s * (a b) + (add ? out : 0) for N x N blocks in shared memory, by 128 threads:
+ * thread t computes rows RB (t / (N / CB)) + [0, RB) and columns CB (t % (N / CB)) + [0, CB),
+ * each entry summed over k in order. */
+template <int N>
+__device__ __forceinline__ void gemm_small(double *out, int ldo, const double *a, int lda, const double *b, int ldb,
+                                           double sgn, bool add) {
+    constexpr int RB = N / 16, CB = N / 8;
+    const int t = threadIdx.x, tr = t / (N / CB), tc = t % (N / CB);
+    double acc[RB][CB];
+#pragma unroll
+    for (int i = 0; i < RB; i++)
+#pragma unroll
+        for (int j = 0; j < CB; j++) acc[i][j] = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < N; k++) {
+        double av[RB], bv[CB];
+#pragma unroll
+        for (int i = 0; i < RB; i++) av[i] = a[(RB * tr + i) * lda + k];
+#pragma unroll
+        for (int j = 0; j < CB; j++) bv[j] = b[k * ldb + CB * tc + j];
+#pragma unroll
+        for (int i = 0; i < RB; i++)
+#pragma unroll
+            for (int j = 0; j < CB; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < RB; i++)
+#pragma unroll
+        for (int j = 0; j < CB; j++) {
+            double *o = out + (RB * tr + i) * ldo + CB * tc + j;
+            *o = add ? *o + sgn * acc[i][j] : sgn * acc[i][j];
+        }
+}
+
+/* in-place inverse of the N x N block at m (ld), N = 32 or 64, by 128 threads; scratch:
+ * 2 (N/2)^2 doubles for this level's W and V and the lower levels' after them */
+template <int N>
+__device__ void inv_block(double *m, int ld, double *scratch) {
+    constexpr int H = N / 2;
+    double *A = m, *B = m + H, *Cb = m + H * ld, *D = m + H * ld + H;
+    double *W = scratch, *V = scratch + H * H, *lower = scratch + 2 * H * H;
+    if constexpr (H == 16) {
+        if (threadIdx.x < 32) inv16_warp(A, ld);
+    } else {
+        inv_block<H>(A, ld, lower);
+    }
+    __syncthreads();
+    gemm_small<H>(W, H, A, ld, B, ld, 1.0, false);   /* W = A^-1 B */
+    gemm_small<H>(V, H, Cb, ld, A, ld, 1.0, false);  /* V = C A^-1 */
+    __syncthreads();
+    gemm_small<H>(D, ld, Cb, ld, W, H, -1.0, true);  /* S = D - C W */
+    __syncthreads();
+    if constexpr (H == 16) {
+        if (threadIdx.x < 32) inv16_warp(D, ld);
+    } else {
+        inv_block<H>(D, ld, lower);
+    }
+    __syncthreads();
+    gemm_small<H>(B, ld, W, H, D, ld, -1.0, false);  /* B = -W S^-1 */
+    gemm_small<H>(Cb, ld, D, ld, V, H, -1.0, false); /* C = -S^-1 V */
+    __syncthreads();
+    gemm_small<H>(A, ld, W, H, Cb, ld, -1.0, true);  /* A = A^-1 - W C */
+    __syncthreads();
+}
+
+/* scratch doubles inv_block<64> needs: 2 * 32^2 + 2 * 16^2 */
+#define GJ_INV_SCRATCH (2 * 32 * 32 + 2 * 16 * 16)
+
 /* P = inv(U[K, :]): the first step's pivot block (later ones are inverted by the update
- * tile that produces them, k_gj_update) */
-__global__ void __launch_bounds__(256) k_gj_diag(const double *__restrict__ U, int k0, double *__restrict__ P) {
-    __shared__ __align__(16) double s_prow[2][GJ_B];
-    const int t = threadIdx.x, r = t >> 2, g = t & 3;
-    double T[16];
-    const double *src = U + (size_t)(k0 + r) * GJ_B + 16 * g;
-#pragma unroll
-    for (int j = 0; j < 16; j++) T[j] = src[j];
-    invert64_regs<256>(T, s_prow);
-    double *dst = P + (size_t)r * GJ_B + 16 * g;
-#pragma unroll
-    for (int j = 0; j < 16; j++) dst[j] = T[j];
+ * tile that produces them, k_gj_update); 128 threads, the block and its scratch in the
+ * same dynamic shared memory as the GEMM kernels */
+__global__ void __launch_bounds__(128) k_gj_diag(const double *__restrict__ U, int k0, double *__restrict__ P) {
+    extern __shared__ __align__(16) double sm[];
+    double *sM = sm, *scr = sm + GJ_B * GJ_LD;
+    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x)
+        sM[(t >> 6) * GJ_LD + (t & 63)] = U[(size_t)(k0 + (t >> 6)) * GJ_B + (t & 63)];
+    __syncthreads();
+    inv_block<64>(sM, GJ_LD, scr);
+    for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) P[t] = sM[(t >> 6) * GJ_LD + (t & 63)];
 }
 
 /* row panel: A[K, J] = P A[K, J] for every 64-column tile J != K (one CTA per tile); the
@@ -234,17 +296,10 @@ __global__ void __launch_bounds__(128) k_gj_update(int n, double *__restrict__ A
             if (pivot_next) *reinterpret_cast<double2 *>(sA + r * GJ_LD + c) = v;
         }
     if (pivot_next) {
-        /* the next pivot block, row-owned (thread t: row t / 2, 32 columns), inverted in place */
-        __shared__ __align__(16) double s_prow[2][GJ_B];
+        /* the next pivot block (now in sA) inverted in place, sB as scratch */
         __syncthreads();
-        const int t = threadIdx.x, r = t >> 1, g = t & 1;
-        double T[32];
-#pragma unroll
-        for (int j = 0; j < 32; j++) T[j] = sA[r * GJ_LD + 32 * g + j];
-        invert64_regs<128>(T, s_prow);
-#pragma unroll
-        for (int j = 0; j < 32; j += 2)
-            *reinterpret_cast<double2 *>(Pn + (size_t)r * GJ_B + 32 * g + j) = make_double2(T[j], T[j + 1]);
+        inv_block<64>(sA, GJ_LD, sB);
+        for (int t = threadIdx.x; t < GJ_B * GJ_B; t += blockDim.x) Pn[t] = sA[(t >> 6) * GJ_LD + (t & 63)];
     }
 }
 
@@ -285,11 +340,12 @@ static int gj_run(int m, double *d_a, cudaStream_t st, double *scratch) {
     if (!attr) {
         cudaFuncSetAttribute(k_gj_row_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_gj_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
     const int nt = m / GJ_B;
     k_gj_copy_col<<<(m * GJ_B + 255) / 256, 256, 0, st>>>(m, d_a, 0, Ub[0]);
-    k_gj_diag<<<1, 256, 0, st>>>(Ub[0], 0, Pb[0]);
+    k_gj_diag<<<1, 128, smem, st>>>(Ub[0], 0, Pb[0]);
     for (int k = 0; k < nt; k++) {
         const int k0 = GJ_B * k;
         double *U = Ub[k & 1], *Un = Ub[(k + 1) & 1];
