@@ -95,9 +95,14 @@ def test_mixed_batch_truncated_matches_fp64_residuals(pkg, graphs):
             assert m.rel_residual <= 1.5 * f.rel_residual + 1e-9, (q, m.rel_residual, f.rel_residual)
 
 
-def test_mixed_batch_converged_matches_fp64(pkg, graphs):
-    """Converged solves: every graph reaches the FP64 tolerance (refinement, or FP64 after
-    a stagnating graph) and the poses agree with the FP64 batch."""
+def test_mixed_batch_converged_matches_fp64(pkg, graphs, oracle):
+    """Converged solves: every graph reaches the FP64 tolerance (refinement, or FP64 for a
+    graph whose refinement stagnates) and each graph's step is as close to the exact
+    solution of its system, in the energy norm, as the FP64 batch's. (Two solves that both
+    meet 1e-8 on these nearly singular systems can differ by cond x tol in the 2-norm, so
+    that norm is not the criterion.)"""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
     opts = dict(tol=1e-8, max_iter=20000, angle_wrap=1, max_refine=200)
     poses = {}
     for prec in (0, 1):
@@ -107,8 +112,20 @@ def test_mixed_batch_converged_matches_fp64(pkg, graphs):
         poses[prec] = [b.graph_poses(q).copy() for q in range(len(graphs))]
         b.close()
     for q, cg in enumerate(graphs):
-        d = np.linalg.norm(poses[1][q] - poses[0][q]) / np.linalg.norm(poses[0][q] - cg.init)
-        assert d <= 1e-5, (q, d)
+        blocks, _ = oracle.se2_linearise(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAMS[q])
+        dim = 3 * cg.n_poses
+        rp, ci, va, xi = oracle.csr_build_anchor(dim, cg.edge_i, cg.edge_j, blocks, 1e6)
+        A = sp.csr_matrix((va, ci, rp), shape=(dim, dim))
+        xs = spl.spsolve(A.tocsc(), xi)
+        scale = np.sqrt(xs @ (A @ xs))
+        if scale < 1e-9:
+            continue  # nothing to solve: the guess is already optimal
+        err = {}
+        for prec in (0, 1):
+            dx = (poses[prec][q] - cg.init).reshape(-1)
+            dx[2::3] = (dx[2::3] + np.pi) % (2 * np.pi) - np.pi
+            err[prec] = np.sqrt(max((dx - xs) @ (A @ (dx - xs)), 0.0))
+        assert err[1] <= max(1e-6 * scale, 3.0 * err[0]), (q, err[1] / scale, err[0] / scale)
 
 
 def test_batch_matches_oracle_per_graph(pkg, graphs, oracle):
