@@ -788,11 +788,13 @@ def run_ncu_case(args):
         g.close()
         return
     if args.ncu_case == "batch":
-        # the 64-graph batch, 20 iterations of each solver (tol 0): one launch per solver
+        # the 64-graph batch, 20 iterations of each solver (tol 0): one launch per solver, in
+        # the launch shape the tuner picks for it (256 threads, two CTAs per SM)
         graphs, lams = c4_batch_graphs()
         for prec in (G.abi.PREC_FP64, G.abi.PREC_MIXED):
             b = G.PoseGraphBatch.from_se2_list(graphs, lams, precision=prec, tol=0.0, max_iter=20,
-                                               inner_max_iter=20, max_refine=1, angle_wrap=1)
+                                               inner_max_iter=20, max_refine=1, angle_wrap=1,
+                                               threads_per_cta=256, ctas_per_sm=2)
             st = b.round_all()
             print(f"batch prec {prec}: {st[0].iterations} iterations, {st[0].solve_ms:.3f} ms", flush=True)
             b.close()

@@ -62,6 +62,31 @@ __device__ __forceinline__ void tv_st(float *v4, int row, TV<float> v) {
     *reinterpret_cast<float4 *>(v4 + 4 * (size_t)row) = make_float4(v.a, v.b, v.c, 0.f);
 }
 
+/* ---- loads of data that each iteration streams once (block values, column indices,
+ * D^-1): read-only, marked evict-first in L2 by a cache policy, so that a batch whose
+ * matrix is larger than L2 streams it without pushing out the solve's vectors (p, z, q,
+ * r, x: gathered by neighbours and reread in the same iteration) ---- */
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ double ld_stream(const double *p, uint64_t pol) {
+    double v;
+    asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float *p, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const int *p, uint64_t pol) {
+    int v;
+    asm volatile("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 /* p = z + beta p_old (first iteration: p = z), as MatrixOps.c:382, for a neighbour row */
 template <typename T>
 __device__ __forceinline__ TV<T> tv_p_of(const T *z4, const T *pold4, int row, T beta, bool first) {
@@ -71,24 +96,30 @@ __device__ __forceinline__ TV<T> tv_p_of(const T *z4, const T *pold4, int row, T
     return { z.a + beta * p.a, z.b + beta * p.b, z.c + beta * p.c };
 }
 
-/* z = D^-1 r with the FP64 block, rounded to T */
+/* z = D^-1 r with the FP64 block (apply_dinv's arithmetic, the block streamed), rounded
+ * to T */
 template <typename T>
-__device__ __forceinline__ TV<T> tv_dinv(const double *dinv, int row, TV<T> r) {
-    const V3 z = apply_dinv(dinv, row, V3{ (double)r.a, (double)r.b, (double)r.c });
-    return { (T)z.a, (T)z.b, (T)z.c };
+__device__ __forceinline__ TV<T> tv_dinv(const double *dinv, int row, TV<T> rv, uint64_t pol) {
+    const double *d = dinv + 288 * (size_t)(row >> 5) + (row & 31);
+    const double ra = rv.a, rb = rv.b, rc = rv.c;
+    double z0 = 0.0, z1 = 0.0, z2 = 0.0;
+    z0 = z0 + ld_stream(d + 0, pol) * ra;   z0 = z0 + ld_stream(d + 32, pol) * rb;  z0 = z0 + ld_stream(d + 64, pol) * rc;
+    z1 = z1 + ld_stream(d + 96, pol) * ra;  z1 = z1 + ld_stream(d + 128, pol) * rb; z1 = z1 + ld_stream(d + 160, pol) * rc;
+    z2 = z2 + ld_stream(d + 192, pol) * ra; z2 = z2 + ld_stream(d + 224, pol) * rb; z2 = z2 + ld_stream(d + 256, pol) * rc;
+    return { (T)z0, (T)z1, (T)z2 };
 }
 
 /* q = A p for one row, blocks in ascending column order (spmv_row for either type) */
 template <typename T>
 __device__ __forceinline__ TV<T> tv_spmv_row(const T *vb, const int *cb, int len, const T *z4, const T *pold,
-                                              T beta, bool first) {
+                                              T beta, bool first, uint64_t pol) {
     T q0 = 0, q1 = 0, q2 = 0;
     int j = 0;
     /* four blocks at a time: their column and neighbour loads are in flight together (the
      * blocks are still added one after another in ascending column order) */
     for (; j + 3 < len; j += 4) {
-        const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
-        const int c2 = __ldg(cb + 32 * (j + 2)), c3 = __ldg(cb + 32 * (j + 3));
+        const int c0 = ld_stream(cb + 32 * j, pol), c1 = ld_stream(cb + 32 * (j + 1), pol);
+        const int c2 = ld_stream(cb + 32 * (j + 2), pol), c3 = ld_stream(cb + 32 * (j + 3), pol);
         const TV<T> p0 = tv_p_of(z4, pold, c0, beta, first), p1 = tv_p_of(z4, pold, c1, beta, first);
         const TV<T> p2 = tv_p_of(z4, pold, c2, beta, first), p3 = tv_p_of(z4, pold, c3, beta, first);
         const TV<T> pp[4] = { p0, p1, p2, p3 };
@@ -96,29 +127,29 @@ __device__ __forceinline__ TV<T> tv_spmv_row(const T *vb, const int *cb, int len
         for (int u = 0; u < 4; u++) {
             const T *v0 = vb + 288 * (j + u);
             const TV<T> pu = pp[u];
-            q0 = q0 + __ldg(v0) * pu.a;       q0 = q0 + __ldg(v0 + 32) * pu.b;  q0 = q0 + __ldg(v0 + 64) * pu.c;
-            q1 = q1 + __ldg(v0 + 96) * pu.a;  q1 = q1 + __ldg(v0 + 128) * pu.b; q1 = q1 + __ldg(v0 + 160) * pu.c;
-            q2 = q2 + __ldg(v0 + 192) * pu.a; q2 = q2 + __ldg(v0 + 224) * pu.b; q2 = q2 + __ldg(v0 + 256) * pu.c;
+            q0 = q0 + ld_stream(v0, pol) * pu.a;       q0 = q0 + ld_stream(v0 + 32, pol) * pu.b;  q0 = q0 + ld_stream(v0 + 64, pol) * pu.c;
+            q1 = q1 + ld_stream(v0 + 96, pol) * pu.a;  q1 = q1 + ld_stream(v0 + 128, pol) * pu.b; q1 = q1 + ld_stream(v0 + 160, pol) * pu.c;
+            q2 = q2 + ld_stream(v0 + 192, pol) * pu.a; q2 = q2 + ld_stream(v0 + 224, pol) * pu.b; q2 = q2 + ld_stream(v0 + 256, pol) * pu.c;
         }
     }
     for (; j + 1 < len; j += 2) {
-        const int c0 = __ldg(cb + 32 * j), c1 = __ldg(cb + 32 * (j + 1));
+        const int c0 = ld_stream(cb + 32 * j, pol), c1 = ld_stream(cb + 32 * (j + 1), pol);
         const TV<T> p0 = tv_p_of(z4, pold, c0, beta, first), p1 = tv_p_of(z4, pold, c1, beta, first);
         const T *v0 = vb + 288 * j, *v1 = v0 + 288;
-        q0 = q0 + __ldg(v0) * p0.a;       q0 = q0 + __ldg(v0 + 32) * p0.b;  q0 = q0 + __ldg(v0 + 64) * p0.c;
-        q1 = q1 + __ldg(v0 + 96) * p0.a;  q1 = q1 + __ldg(v0 + 128) * p0.b; q1 = q1 + __ldg(v0 + 160) * p0.c;
-        q2 = q2 + __ldg(v0 + 192) * p0.a; q2 = q2 + __ldg(v0 + 224) * p0.b; q2 = q2 + __ldg(v0 + 256) * p0.c;
-        q0 = q0 + __ldg(v1) * p1.a;       q0 = q0 + __ldg(v1 + 32) * p1.b;  q0 = q0 + __ldg(v1 + 64) * p1.c;
-        q1 = q1 + __ldg(v1 + 96) * p1.a;  q1 = q1 + __ldg(v1 + 128) * p1.b; q1 = q1 + __ldg(v1 + 160) * p1.c;
-        q2 = q2 + __ldg(v1 + 192) * p1.a; q2 = q2 + __ldg(v1 + 224) * p1.b; q2 = q2 + __ldg(v1 + 256) * p1.c;
+        q0 = q0 + ld_stream(v0, pol) * p0.a;       q0 = q0 + ld_stream(v0 + 32, pol) * p0.b;  q0 = q0 + ld_stream(v0 + 64, pol) * p0.c;
+        q1 = q1 + ld_stream(v0 + 96, pol) * p0.a;  q1 = q1 + ld_stream(v0 + 128, pol) * p0.b; q1 = q1 + ld_stream(v0 + 160, pol) * p0.c;
+        q2 = q2 + ld_stream(v0 + 192, pol) * p0.a; q2 = q2 + ld_stream(v0 + 224, pol) * p0.b; q2 = q2 + ld_stream(v0 + 256, pol) * p0.c;
+        q0 = q0 + ld_stream(v1, pol) * p1.a;       q0 = q0 + ld_stream(v1 + 32, pol) * p1.b;  q0 = q0 + ld_stream(v1 + 64, pol) * p1.c;
+        q1 = q1 + ld_stream(v1 + 96, pol) * p1.a;  q1 = q1 + ld_stream(v1 + 128, pol) * p1.b; q1 = q1 + ld_stream(v1 + 160, pol) * p1.c;
+        q2 = q2 + ld_stream(v1 + 192, pol) * p1.a; q2 = q2 + ld_stream(v1 + 224, pol) * p1.b; q2 = q2 + ld_stream(v1 + 256, pol) * p1.c;
     }
     if (j < len) {
-        const int c0 = __ldg(cb + 32 * j);
+        const int c0 = ld_stream(cb + 32 * j, pol);
         const TV<T> p0 = tv_p_of(z4, pold, c0, beta, first);
         const T *v0 = vb + 288 * j;
-        q0 = q0 + __ldg(v0) * p0.a;       q0 = q0 + __ldg(v0 + 32) * p0.b;  q0 = q0 + __ldg(v0 + 64) * p0.c;
-        q1 = q1 + __ldg(v0 + 96) * p0.a;  q1 = q1 + __ldg(v0 + 128) * p0.b; q1 = q1 + __ldg(v0 + 160) * p0.c;
-        q2 = q2 + __ldg(v0 + 192) * p0.a; q2 = q2 + __ldg(v0 + 224) * p0.b; q2 = q2 + __ldg(v0 + 256) * p0.c;
+        q0 = q0 + ld_stream(v0, pol) * p0.a;       q0 = q0 + ld_stream(v0 + 32, pol) * p0.b;  q0 = q0 + ld_stream(v0 + 64, pol) * p0.c;
+        q1 = q1 + ld_stream(v0 + 96, pol) * p0.a;  q1 = q1 + ld_stream(v0 + 128, pol) * p0.b; q1 = q1 + ld_stream(v0 + 160, pol) * p0.c;
+        q2 = q2 + ld_stream(v0 + 192, pol) * p0.a; q2 = q2 + ld_stream(v0 + 224, pol) * p0.b; q2 = q2 + ld_stream(v0 + 256, pol) * p0.c;
     }
     return { q0, q1, q2 };
 }
@@ -142,6 +173,7 @@ template <> struct BVec<float> {
 template <int BS, typename T>
 __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B) {
     const BVec<T> V(P, B);
+    const uint64_t pol = l2_evict_first_policy();
     extern __shared__ __align__(16) double s_part[]; /* [slices of this CTA][2] */
     __shared__ double s_rz[BATCH_LG_MAX], s_rr[BATCH_LG_MAX], s_bn[BATCH_LG_MAX];
     __shared__ double s_alpha[BATCH_LG_MAX], s_beta[BATCH_LG_MAX];
@@ -211,7 +243,7 @@ __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B)
             const TV<T> b = tv_ldg(V.b, row);
             tv_st(V.x, row, TV<T>{ 0, 0, 0 });
             tv_st(V.r, row, b);
-            const TV<T> z = tv_dinv(P.dinv, row, b);
+            const TV<T> z = tv_dinv(P.dinv, row, b, pol);
             tv_st(V.z, row, z);
             const double b0 = b.a, b1 = b.b, b2 = b.c;
             rz = rz + b0 * (double)z.a; rz = rz + b1 * (double)z.b; rz = rz + b2 * (double)z.c;
@@ -256,7 +288,7 @@ __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B)
                 tv_st(pnew, row, pn);
                 const int64_t sb = __ldg(P.slice_ptr + s);
                 const TV<T> q = tv_spmv_row(V.val + 9 * sb + lane, P.col + sb + lane, __ldg(P.row_len + row), V.z,
-                                            pold, beta, first);
+                                            pold, beta, first, pol);
                 tv_st(V.q, row, q);
                 pq = pq + (double)pn.a * (double)q.a; pq = pq + (double)pn.b * (double)q.b;
                 pq = pq + (double)pn.c * (double)q.c;
@@ -300,7 +332,7 @@ __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B)
                 tv_st(V.r, row, r);
                 const double r0 = r.a, r1 = r.b, r2 = r.c;
                 rr = rr + r0 * r0; rr = rr + r1 * r1; rr = rr + r2 * r2;
-                const TV<T> z = tv_dinv(P.dinv, row, r);
+                const TV<T> z = tv_dinv(P.dinv, row, r, pol);
                 tv_st(V.z, row, z);
                 rz = rz + r0 * (double)z.a; rz = rz + r1 * (double)z.b; rz = rz + r2 * (double)z.c;
             }
