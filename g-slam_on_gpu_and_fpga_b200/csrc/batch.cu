@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B)
                 } else {
                     s_beta[t] = s_tot[1][t] / s_rz[t];
                     s_rz[t] = s_tot[1][t];
+                    if (B.cap != nullptr && k >= __ldg(B.cap + g0 + t)) s_done[t] = GSLAM_STOP_MAXIT + 1;
                 }
             }
             count_done(t);

@@ -291,10 +291,12 @@ int batch_solve(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats 
  * Mixed-precision batch: iterative refinement driven from the host, every graph at
  * once. Per step: the FP32 right-hand side (the FP64 residual, 0 for graphs already
  * done), one launch of the batched PCG in FP32 (FP32 values and vectors, FP64 D^-1 and
- * dot products, per-graph scalars, inner tolerance inner_tol), x += d in FP64, and the
- * FP64 residual b - A x with per-graph norms. A graph stops at tol, at max_iter inner
- * iterations, or when a step does not halve its residual; if any graph stagnates the
- * batch is solved again in FP64 and those results are reported.
+ * dot products, per-graph scalars, inner tolerance inner_tol, each graph capped by what
+ * is left of its max_iter), x += d in FP64, and the FP64 residual b - A x with per-graph
+ * norms. A graph stops at tol, at max_iter inner iterations, or when a whole inner pass
+ * (not one cut short by what is left of max_iter) did not halve the graph's residual
+ * (stagnation); the graphs that stagnate are solved again in FP64 and those results are
+ * reported.
  */
 static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam_solve_stats *total) {
     BatchState &B = *g->batch;
@@ -311,6 +313,7 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
     if (!B.d_bf4) {
         CK(dalloc(m, &B.d_bf4, 4 * 32 * (size_t)L->n_slices));
         CK(dalloc(m, &B.d_gactive, (size_t)G));
+        CK(dalloc(m, &B.d_gcap, (size_t)G));
         CK(dalloc(m, &B.d_gres, (size_t)G));
         CK(cudaMallocHost(&B.h_gres, G * sizeof(double)));
     }
@@ -322,7 +325,7 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
     CK(cudaMemcpyAsync(B.h_gres, B.d_gres, G * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     std::vector<double> bnorm(G), rel(G, 1.0);
-    std::vector<int> its(G, 0), refs(G, 0), reason(G, GSLAM_STOP_MAXIT), active(G, 1);
+    std::vector<int> its(G, 0), refs(G, 0), reason(G, GSLAM_STOP_MAXIT), active(G, 1), cap(G, 0);
     bool stagnated = false;
     for (int q = 0; q < G; q++) {
         bnorm[q] = std::sqrt(B.h_gres[q]);
@@ -359,16 +362,22 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
     BP.res = B.d_res;
     BP.active = B.d_active;
     BP.bf4 = B.d_bf4;
+    BP.cap = B.d_gcap;
     CK(record_event(L->ev0, st));
     for (int step = 0; step < std::max(g->o.max_refine, 1); step++) {
-        int n_active = 0, used = 0;
-        for (int q = 0; q < G; q++)
-            if (active[q]) { n_active++; used = std::max(used, its[q]); }
+        /* each graph's inner pass is capped by what is left of its own budget */
+        int n_active = 0, cap_max = 0;
+        for (int q = 0; q < G; q++) {
+            if (!active[q]) { cap[q] = 0; continue; }
+            cap[q] = std::min(g->o.inner_max_iter, g->o.max_iter - its[q]);
+            if (cap[q] <= 0) { active[q] = 0; reason[q] = GSLAM_STOP_MAXIT; continue; }
+            n_active++;
+            cap_max = std::max(cap_max, cap[q]);
+        }
         if (n_active == 0) break;
-        const int cap = std::min(g->o.inner_max_iter, g->o.max_iter - used);
-        if (cap <= 0) break;
-        P.max_iter = cap;
+        P.max_iter = cap_max;
         CK(cudaMemcpyAsync(B.d_gactive, active.data(), G * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(B.d_gcap, cap.data(), G * sizeof(int), cudaMemcpyHostToDevice, st));
         launch_batch_rhs32(st, L->n_rows, B.d_slice_graph, B.d_gactive, L->r4, B.d_bf4);
         CK(cudaMemsetAsync(L->gs, 0, sizeof(GridSync), st));
         CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
@@ -395,7 +404,14 @@ static int batch_solve_mixed(gslam_graph *g, gslam_solve_stats *per_graph, gslam
             rel[q] = std::sqrt(B.h_gres[q]) / bnorm[q];
             if (rel[q] < g->o.tol) { active[q] = 0; reason[q] = GSLAM_STOP_TOL; }
             else if (its[q] >= g->o.max_iter || refs[q] >= g->o.max_refine) { active[q] = 0; reason[q] = GSLAM_STOP_MAXIT; }
-            else if (rel[q] > 0.5 * prev) { active[q] = 0; reason[q] = GSLAM_STOP_STAGNATION; stagnated = true; }
+            else if (rel[q] > 0.5 * prev && !(B.h_res[q].reason == GSLAM_STOP_MAXIT && cap[q] < g->o.inner_max_iter)) {
+                /* a whole inner pass (to its tolerance or its inner_max_iter) did not halve the
+                 * FP64 residual: FP32 cannot resolve this graph. A pass cut short by what was
+                 * left of the graph's max_iter is not this. */
+                active[q] = 0;
+                reason[q] = GSLAM_STOP_STAGNATION;
+                stagnated = true;
+            }
         }
     }
     CK(record_event(L->ev1, st));

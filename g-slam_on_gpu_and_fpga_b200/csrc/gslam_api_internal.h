@@ -78,6 +78,7 @@ struct BatchState {
     /* mixed batches: FP32 right-hand side, per-graph active flags and residual norms */
     float *d_bf4 = nullptr;
     int *d_gactive = nullptr;
+    int *d_gcap = nullptr;       /* mixed: each graph's iteration cap for the current inner pass */
     double *d_gres = nullptr, *h_gres = nullptr;
     int *d_skip = nullptr;       /* graphs the FP64 rerun of a stagnated mixed batch leaves alone */
     /* chunk sums of the per-graph norm kernels */

@@ -124,6 +124,9 @@ struct BatchParams {
     const int *skip;         /* [n_graphs] or null: graphs left exactly as they are (done from the
                               * start, their vectors untouched: the mixed batch's FP64 rerun of
                               * only the graphs that stagnated) */
+    const int *cap;          /* [n_graphs] or null: each graph's own iteration cap (at most the
+                              * launch's max_iter; the mixed batch's inner passes, each graph
+                              * with what is left of its budget) */
 };
 /* fp32: the inner solve of the mixed batch (FP32 values / vectors in PcgParams' FP32
  * fields, right-hand side bf4); otherwise the FP64 PCG on val / b4. */

@@ -30,7 +30,8 @@ def autotune_batch(graphs, lams, iters: int = 40, candidates=None, cache: str | 
     timings = [(candidate, us_per_iteration or None if it could not run)].
 
     `cache`: a JSON file; a result stored there for the same batch shape is reused."""
-    key = f"{len(graphs)}:{sum(int(g.init.shape[0]) for g in graphs)}:{sum(len(g.edge_i) for g in graphs)}"
+    key = (f"{len(graphs)}:{sum(int(g.init.shape[0]) for g in graphs)}:{sum(len(g.edge_i) for g in graphs)}"
+           f":{opts.get('precision', abi.PREC_FP64)}")
     if cache and os.path.exists(cache):
         with open(cache) as f:
             hit = json.load(f).get(key)
