@@ -25,6 +25,7 @@ ERR_NO_DEVICE = -6
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_FP64_CG = 2   # FP64 PCG, one grid reduction per iteration (Chronopoulos-Gear)
 
 STOP_TOL, STOP_MAXIT, STOP_PQ_ZERO, STOP_TIMEOUT = 0, 1, 2, 3
 

@@ -166,6 +166,7 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
      * values plus its own rows' D^-1 and halo, each up to the shared-memory budget */
     L->resident = false;
     L->mixed_ok = false;
+    L->cg_ok = false;
     const int rgrid = std::min(pcg_resident_max_grid(device, GSLAM_RES_SMEM_MAX),
                                pcg_mixed_max_grid(device, GSLAM_RES_SMEM_MAX));
     if (rgrid > 0 && S.n_slices <= 32 * rgrid) {
@@ -265,7 +266,20 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 L->mixed_stage_off = L->mixed_halo_off + z_bytes;
                 L->mixed_smem_bytes = (size_t)(L->mixed_stage_off + stage_bytes);
             }
-            if (L->resident || L->mixed_ok) {
+            /* FP64 one-reduction solver: FP64 values | local columns | z of own and halo rows
+             * (32 B each) | u, v of the first `block` halo rows (64 B each); D^-1 stays in
+             * global memory (L2), leaving the shared memory to the values */
+            const int64_t z64_bytes = (32 * p_cap + 127) / 128 * 128;
+            const int64_t stage64_bytes = (64 * (int64_t)std::min(h_max, block) + 127) / 128 * 128;
+            const int64_t cap_cg = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes - z64_bytes - stage64_bytes) / 8 / 288 * 288;
+            if (cap_cg >= 0) {
+                L->cg_ok = true;
+                L->cg_val_cap = std::min<int64_t>(cap_cg, 9 * max_slots);
+                L->cg_halo_off = 8 * L->cg_val_cap + col_bytes;
+                L->cg_stage_off = L->cg_halo_off + z64_bytes;
+                L->cg_smem_bytes = (size_t)(L->cg_stage_off + stage64_bytes);
+            }
+            if (L->resident || L->mixed_ok || L->cg_ok) {
                 CK(dupload(m, st, &L->lcol, lcol));
                 CK(dupload(m, st, &L->halo_ptr, hptr));
                 /* only rows that some CTA reads as halo are published in global memory */
@@ -347,12 +361,29 @@ static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts 
     CK(cudaMemsetAsync(L->gs, 0, sizeof(GridSync), st));
     CK(cudaMemsetAsync(L->res, 0, sizeof(PcgResult), st));
     const bool mixed = fused_prec == GSLAM_PREC_MIXED;
+    const bool cg = fused_prec == GSLAM_PREC_FP64_CG;
     if (mixed && !L->mixed_ok) {
         g_last_error = "mixed precision needs the graph's rows to fit the resident layout (<= 32 slices per SM)";
         return GSLAM_ERR_TOO_LARGE;
     }
-    const bool resident = !mixed && L->resident && !o.disable_resident;
-    const int grid = (resident || mixed) ? L->res_grid : L->grid;
+    if (cg && !L->cg_ok) {
+        g_last_error = "the one-reduction FP64 solver needs the graph's rows to fit the resident layout (<= 32 slices per SM)";
+        return GSLAM_ERR_TOO_LARGE;
+    }
+    if (cg) {
+        if (!L->w4) {
+            const size_t nvec = 4 * 32 * (size_t)L->n_slices;
+            CK(dalloc(L->mem, &L->w4, nvec));
+            CK(cudaMemsetAsync(L->w4, 0, nvec * sizeof(double), st));
+        }
+        P.w4 = L->w4;
+        /* one inner solve to the outer tolerance and iteration cap, no refinement */
+        P.inner_tol = o.tol;
+        P.inner_max_iter = o.max_iter;
+        P.max_refine = 1;
+    }
+    const bool resident = !mixed && !cg && L->resident && !o.disable_resident;
+    const int grid = (resident || mixed || cg) ? L->res_grid : L->grid;
     {
         /* 2 barriers per iteration + 1: the arrival counter must not wrap */
         const double barriers = 2.0 * (double)std::max(o.max_iter, 0) + 4.0 * (double)std::max(o.max_refine, 1) + 4.0;
@@ -362,10 +393,10 @@ static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts 
         }
     }
     P.cta_slice = L->cta_slice;
-    P.smem_val_cap = mixed ? L->mixed_val_cap : L->smem_val_cap;
+    P.smem_val_cap = mixed ? L->mixed_val_cap : cg ? L->cg_val_cap : L->smem_val_cap;
     P.smem_dinv_off = L->mixed_dinv_off;
-    P.smem_halo_off = L->mixed_halo_off;
-    P.smem_stage_off = L->mixed_stage_off;
+    P.smem_halo_off = cg ? L->cg_halo_off : L->mixed_halo_off;
+    P.smem_stage_off = cg ? L->cg_stage_off : L->mixed_stage_off;
     P.lcol = L->lcol;
     P.halo_ptr = L->halo_ptr;
     P.halo_rows = L->halo_rows;
@@ -373,7 +404,8 @@ static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts 
     P.smem_p_off = L->smem_p_off;
     tr.step("memsets");
     CK(record_event(L->ev0, st));
-    if (mixed) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->mixed_smem_bytes));
+    if (mixed) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->mixed_smem_bytes, false));
+    else if (cg) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->cg_smem_bytes, true));
     else if (resident) CK(launch_pcg_resident(st, P, grid, L->res_block, L->smem_bytes));
     else CK(launch_pcg(st, P, fused_prec, grid, L->block));
     tr.step("solver launch");

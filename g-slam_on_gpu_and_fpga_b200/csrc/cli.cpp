@@ -64,7 +64,9 @@ int main(int argc, char *argv[]) {
     gslam_opts_default(&o);
     if (const char *s = getenv("GSLAM_TOL")) o.tol = atof(s);
     if (const char *s = getenv("GSLAM_MAXIT")) o.max_iter = atoi(s);
-    if (const char *s = getenv("GSLAM_PREC")) o.precision = (strcmp(s, "mixed") == 0) ? GSLAM_PREC_MIXED : GSLAM_PREC_FP64;
+    if (const char *s = getenv("GSLAM_PREC"))
+        o.precision = (strcmp(s, "mixed") == 0) ? GSLAM_PREC_MIXED
+                    : (strcmp(s, "fp64cg") == 0) ? GSLAM_PREC_FP64_CG : GSLAM_PREC_FP64;
     if (const char *s = getenv("GSLAM_WRAP")) o.angle_wrap = atoi(s);
     const bool stats_json = getenv("GSLAM_STATS") && atoi(getenv("GSLAM_STATS"));
 

@@ -52,6 +52,11 @@ struct DevLayout {
     int64_t mixed_dinv_off = 0, mixed_halo_off = 0;
     int64_t mixed_stage_off = 0;     /* halo u, v staging (cp.async) */
     size_t mixed_smem_bytes = 0;
+    bool cg_ok = false;             /* the FP64 one-reduction solver's layout fits */
+    int64_t cg_val_cap = 0;        /* doubles staged per CTA */
+    int64_t cg_halo_off = 0, cg_stage_off = 0;
+    size_t cg_smem_bytes = 0;
+    double *w4 = nullptr;          /* its sixth published vector (made on first use) */
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;   /* brackets the solver launch */
     int max_grid_alloc() const { return partial_capacity; }
 };

@@ -65,6 +65,7 @@ struct PcgParams {
     const double *dinv;    /* block-Jacobi inverses (slot layout) */
     const double *b4;      /* right-hand side, padded new order */
     double *x4, *r4, *z4, *p4a, *p4b, *q4;  /* FP64 work vectors */
+    double *w4;            /* FP64 one-reduction solver: its sixth published vector */
     float *xf4, *rf4, *zf4, *pfa4, *pfb4, *qf4; /* FP32 work vectors (mixed) */
     double tol_rel;
     int max_iter;
@@ -157,8 +158,10 @@ cudaError_t launch_pcg_resident(cudaStream_t st, const PcgParams &p, int grid, i
                                 size_t smem_bytes);
 int pcg_resident_max_grid(int device, size_t smem_bytes);
 
-/* Mixed-precision solver (pcg_mixed.cu). */
-cudaError_t launch_pcg_mixed(cudaStream_t st, const PcgParams &p, int grid, int block, size_t smem_bytes);
+/* Mixed-precision solver (pcg_mixed.cu); fp64: the same kernel as the FP64 one-reduction
+ * solver. */
+cudaError_t launch_pcg_mixed(cudaStream_t st, const PcgParams &p, int grid, int block, size_t smem_bytes,
+                             bool fp64);
 int pcg_mixed_max_grid(int device, size_t smem_bytes);
 
 /* Standalone SpMV y = A x on padded new-order vectors (FP64 or FP32 values). */

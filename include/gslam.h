@@ -35,6 +35,10 @@ extern "C" {
 /* ---- solver precision ---- */
 #define GSLAM_PREC_FP64 0  /* FP64 block-Jacobi PCG (the reference's arithmetic) */
 #define GSLAM_PREC_MIXED 1 /* FP32 SpMV / vectors inside FP64 iterative refinement */
+#define GSLAM_PREC_FP64_CG 2 /* FP64 block-Jacobi PCG with one grid reduction per iteration
+                              * (Chronopoulos-Gear recurrence: the reference's iterates in exact
+                              * arithmetic, other rounding); the graph must fit the resident
+                              * layout (<= 32 slices per SM). Batches solve it as FP64. */
 
 /* ---- factor families ---- */
 #define GSLAM_FACTORS_REFERENCE 0 /* ObsEdge + MotionEdge of src/cpu_pcg_fp64 */
