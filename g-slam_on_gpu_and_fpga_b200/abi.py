@@ -32,7 +32,7 @@ STOP_TOL, STOP_MAXIT, STOP_PQ_ZERO, STOP_TIMEOUT = 0, 1, 2, 3
 # every extern "C" symbol the headers declare (checked by the CPU tests)
 EXPORTS = [
     "gslam_opts_default", "gslam_create_reference", "gslam_create_se2", "gslam_destroy",
-    "gslam_set_opts", "gslam_sizes", "gslam_get_stream", "gslam_set_poses", "gslam_get_poses", "gslam_round",
+    "gslam_set_opts", "gslam_sizes", "gslam_get_stream", "gslam_set_poses", "gslam_get_poses", "gslam_round", "gslam_round_io",
     "gslam_run", "gslam_linearise", "gslam_assemble", "gslam_solve", "gslam_update",
     "gslam_get_edge_blocks", "gslam_assemble_from_edges", "gslam_get_csr", "gslam_get_dx",
     "gslam_get_diag_inv", "gslam_spmv", "gslam_spmv_bench", "gslam_spmv_bytes", "gslam_read_log", "gslam_free_log",
@@ -130,6 +130,7 @@ def lib() -> C.CDLL:
             "gslam_set_poses": [VP, DP],
             "gslam_get_poses": [VP, DP],
             "gslam_round": [VP, C.POINTER(SolveStats)],
+            "gslam_round_io": [VP, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(SolveStats)],
             "gslam_run": [VP, C.c_int, DP, IP],
             "gslam_linearise": [VP],
             "gslam_assemble": [VP],

@@ -814,12 +814,18 @@ static int round_graph_build(gslam_graph *g) {
 }
 
 /* one round replayed from the captured graph (gslam_opts.round_graph) */
-static int round_graphed(gslam_graph *g, gslam_solve_stats *stats) {
+/* one replay of the captured round; poses_in / poses_out (host, may be NULL) are copied in
+ * before it and out after it on the same stream, so the whole step waits once */
+static int round_graphed(gslam_graph *g, gslam_solve_stats *stats, const double *poses_in = nullptr,
+                         double *poses_out = nullptr) {
     if (!g->round_exec) {
         const int rc = round_graph_build(g);
         if (rc != GSLAM_OK) return rc;
     }
+    const size_t pose_bytes = 3 * (size_t)g->n_poses * sizeof(double);
+    if (poses_in) CK(cudaMemcpyAsync(g->d_poses, poses_in, pose_bytes, cudaMemcpyHostToDevice, g->st));
     CK(cudaGraphLaunch(g->round_exec, g->st));
+    if (poses_out) CK(cudaMemcpyAsync(poses_out, g->d_poses, pose_bytes, cudaMemcpyDeviceToHost, g->st));
     CK(cudaStreamSynchronize(g->st));
     gslam_solve_stats st;
     memset(&st, 0, sizeof st);
@@ -828,12 +834,28 @@ static int round_graphed(gslam_graph *g, gslam_solve_stats *stats) {
     double diff = *g->h_diff;
     int rc = layout_solve_finish(&g->L, g->st, g->o, g->h_res, &st);
     g->last_res = *g->h_res;
-    if (rc == GSLAM_OK && stagnated) rc = gslam_update_ex(g, &diff, g->ev_round1);
+    if (rc == GSLAM_OK && stagnated) {
+        /* the FP64 re-solve moved the poses after the copy-out: copy them again */
+        rc = gslam_update_ex(g, &diff, g->ev_round1);
+        if (rc == GSLAM_OK && poses_out) rc = gslam_get_poses(g, poses_out);
+    }
     float ms = 0.f;
     if (rc == GSLAM_OK) ms = elapsed_ms(g->ev_round0, g->ev_round1);
     st.diff = diff;
     st.round_ms = ms;
     if (stats) *stats = st;
+    return rc;
+}
+
+int gslam_round_io(gslam_graph *g, const double *poses_in, double *poses_out, gslam_solve_stats *stats) {
+    if (!g) BAD("null handle");
+    if (g->o.round_graph && !g->batch && g->eager_rounds > 0 && g->ev_round0)
+        return round_graphed(g, stats, poses_in, poses_out);
+    /* the eager round (the first, or without round_graph): the separate calls */
+    int rc = GSLAM_OK;
+    if (poses_in) rc = gslam_set_poses(g, poses_in);
+    if (rc == GSLAM_OK) rc = gslam_round(g, stats);
+    if (rc == GSLAM_OK && poses_out) rc = gslam_get_poses(g, poses_out);
     return rc;
 }
 

@@ -180,6 +180,20 @@ class PoseGraph:
         return RoundStats(st.iterations, st.refinements, st.reason, st.rel_residual, st.diff, st.solve_ms,
                           st.round_ms)
 
+    def round_io(self, poses_in=None, poses_out=None) -> RoundStats:
+        """One round with host input and output (gslam_round_io): poses_in (N x 3 float64,
+        or None to keep the device poses) in, the round, the new poses into poses_out (N x 3
+        float64, or None); one wait. Pass page-locked arrays (e.g. torch pin_memory) for
+        asynchronous copies."""
+        dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        for a in (poses_in, poses_out):
+            if a is not None and (a.dtype != np.float64 or a.shape != (self.n_poses, 3) or not a.flags.c_contiguous):
+                raise ValueError("poses must be a C-contiguous (n_poses, 3) float64 array")
+        st = abi.SolveStats()
+        abi.check(abi.lib().gslam_round_io(self._h, dp(poses_in), dp(poses_out), C.byref(st)))
+        return RoundStats(st.iterations, st.refinements, st.reason, st.rel_residual, st.diff, st.solve_ms,
+                          st.round_ms)
+
     def stream(self) -> int:
         """The cudaStream_t (as an int) all work on this graph runs on."""
         s = C.c_void_p()

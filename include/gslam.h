@@ -146,6 +146,15 @@ int gslam_get_poses(gslam_graph *g, double *poses);
 int gslam_round(gslam_graph *g, gslam_solve_stats *stats);
 
 /*
+ * One round with its input and output in host memory: poses_in (3 doubles per pose, may
+ * be NULL to keep the device poses) is copied in, the round runs, and the new poses are
+ * copied to poses_out (may be NULL), all on the graph's stream with one wait at the end
+ * (round_graph on, after the first round; otherwise the same as gslam_set_poses,
+ * gslam_round, gslam_get_poses). Pinned host buffers make the copies asynchronous.
+ */
+int gslam_round_io(gslam_graph *g, const double *poses_in, double *poses_out, gslam_solve_stats *stats);
+
+/*
  * Up to max_rounds rounds with the reference's stop rules (diff < 0.01, or 20
  * rounds without a new best diff). diffs[max_rounds] (may be NULL) receives the
  * per-round diff; *rounds_done the number executed.

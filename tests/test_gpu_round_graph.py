@@ -78,3 +78,31 @@ def test_round_graph_rebuilt_after_set_opts(pkg, synth):
             runs.append((a + b, p))
     assert runs[0][0] == runs[1][0]
     assert_bitwise(runs[1][1], runs[0][1], "poses")
+
+
+def test_round_io_matches_separate_calls(pkg):
+    """gslam_round_io (poses in, round, poses out on the graph's stream, one wait) gives the
+    poses of gslam_set_poses + gslam_round + gslam_get_poses, bit for bit, in the eager
+    first round and in graph replays."""
+    import numpy as np
+    synth = importlib.import_module("g-slam_on_gpu_and_fpga_b200.synth")
+    cg = synth.city_grid(3000, seed=12)
+    out = {}
+    for mode in ("io", "separate"):
+        with pkg.PoseGraph.from_se2(cg.init, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam=0.1, angle_wrap=1,
+                                    round_graph=1) as g:
+            p = np.ascontiguousarray(cg.init, np.float64)
+            res = []
+            for _ in range(4):
+                if mode == "io":
+                    q = np.empty_like(p)
+                    g.round_io(p, q)
+                else:
+                    g.poses = p
+                    g.round()
+                    q = g.poses
+                res.append(q.copy())
+                p = q
+            out[mode] = res
+    for a, b in zip(out["io"], out["separate"]):
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
