@@ -205,21 +205,18 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
         std::vector<int> cs(rgrid + 1);
         fill(lo, &cs);
         bool ok = cs[0] == 0 && cs[rgrid] == S.n_slices;
-        int64_t max_slots = 0;
-        for (int i = 0; i < rgrid; i++) {
+        for (int i = 0; i < rgrid; i++)
             if (cs[i + 1] < cs[i] || cs[i + 1] - cs[i] > cap_sl) ok = false;
-            max_slots = std::max(max_slots, S.slice_ptr[cs[i + 1]] - S.slice_ptr[cs[i]]);
-        }
         if (ok) {
             L->res_grid = rgrid;
             L->res_block = block;
             CK(dupload(m, st, &L->cta_slice, cs));
             L->partial_capacity = std::max(L->partial_capacity, rgrid);
-            const int64_t col_bytes = (4 * max_slots + 127) / 128 * 128;
             /* CTA-local column indices (own rows first, then the CTA's halo) and halo lists */
             std::vector<int> lcol(S.n_slots, 0), hptr(rgrid + 1, 0), hrows;
-            int64_t p_cap = 0;
-            int sl_max = 0, h_max = 0;
+            /* mixed / FP64 one-reduction solvers: every CTA's own layout must fit */
+            bool fit32 = true, fit64 = true, fit_res = true;
+            int64_t cap32_min = INT64_MAX, cap64_min = INT64_MAX, cap_res_min = INT64_MAX;
             for (int i = 0; i < rgrid; i++) {
                 const int row0 = 32 * cs[i], row1 = 32 * cs[i + 1], nloc = row1 - row0;
                 const int64_t a0 = S.slice_ptr[cs[i]], a1 = S.slice_ptr[cs[i + 1]];
@@ -238,46 +235,41 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 }
                 hptr[i + 1] = hptr[i] + (int)rem.size();
                 hrows.insert(hrows.end(), rem.begin(), rem.end());
-                p_cap = std::max<int64_t>(p_cap, nloc + (int64_t)rem.size());
-                sl_max = std::max(sl_max, cs[i + 1] - cs[i]);
-                h_max = std::max(h_max, (int)rem.size());
+                const MixedSmem l32 = mixed_smem_layout(4, false, a1 - a0, cs[i + 1] - cs[i], (int64_t)rem.size(), block,
+                                                        GSLAM_RES_SMEM_MAX);
+                const MixedSmem l64 = mixed_smem_layout(8, true, a1 - a0, cs[i + 1] - cs[i], (int64_t)rem.size(), block,
+                                                        GSLAM_RES_SMEM_MAX);
+                const ResidentSmem lr = resident_smem_layout(a1 - a0, cs[i + 1] - cs[i], (int64_t)rem.size(),
+                                                             GSLAM_RES_SMEM_MAX);
+                fit_res = fit_res && lr.val_cap >= 0;
+                cap_res_min = std::min(cap_res_min, std::min<int64_t>(lr.val_cap, 9 * (a1 - a0)));
+                fit32 = fit32 && l32.val_cap >= 0;
+                fit64 = fit64 && l64.val_cap >= 0;
+                cap32_min = std::min(cap32_min, std::min<int64_t>(l32.val_cap, 9 * (a1 - a0)));
+                cap64_min = std::min(cap64_min, std::min<int64_t>(l64.val_cap, 9 * (a1 - a0)));
             }
-            /* FP64: values | local columns | staged p (32 B per own or halo row) */
-            const int64_t p_bytes = 32 * p_cap;
-            const int64_t cap64 = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes - p_bytes) / 8 / 288 * 288;
-            if (cap64 >= 0 && !o.disable_resident) {
+            /* FP64: values | local columns | staged p (32 B per own or halo row), each CTA's
+             * from its own sizes (resident_smem_layout) */
+            if (fit_res && !o.disable_resident) {
                 L->resident = true;
-                L->smem_val_cap = std::min<int64_t>(cap64, 9 * max_slots);
-                L->smem_p_off = 8 * L->smem_val_cap + col_bytes;
-                L->smem_bytes = (size_t)(L->smem_p_off + p_bytes);
+                L->smem_val_cap = cap_res_min; /* the smallest CTA's share (statistics only) */
+                L->smem_bytes = GSLAM_RES_SMEM_MAX;
             }
-            /* mixed: FP32 values | local columns | D^-1 of own rows (2304 B per slice) |
-             * z of own and halo rows (16 B each) | u, v of the first `block` halo rows
-             * (32 B each, copied in asynchronously) */
-            const int64_t z_bytes = (16 * p_cap + 127) / 128 * 128;
-            const int64_t stage_bytes = (32 * (int64_t)std::min(h_max, block) + 127) / 128 * 128;
-            const int64_t fixed = col_bytes + 2304 * (int64_t)sl_max + z_bytes + stage_bytes;
-            const int64_t cap32 = ((int64_t)GSLAM_RES_SMEM_MAX - fixed) / 4 / 288 * 288;
-            if (cap32 >= 0) {
+            /* mixed: FP32 values | local columns | D^-1 of own rows (2304 B per slice) | z of
+             * own and halo rows (16 B each) | u, v of the first `block` halo rows (32 B each,
+             * copied in asynchronously); FP64 one-reduction solver: FP64 values | local
+             * columns | z (32 B per row) | u, v (64 B per halo row), D^-1 in global memory
+             * (L2). Each CTA lays its share out from its own sizes (mixed_smem_layout), so a
+             * CTA with a short halo keeps more of its values on chip. */
+            if (fit32) {
                 L->mixed_ok = true;
-                L->mixed_val_cap = std::min<int64_t>(cap32, 9 * max_slots);
-                L->mixed_dinv_off = 4 * L->mixed_val_cap + col_bytes;
-                L->mixed_halo_off = L->mixed_dinv_off + 2304 * (int64_t)sl_max;
-                L->mixed_stage_off = L->mixed_halo_off + z_bytes;
-                L->mixed_smem_bytes = (size_t)(L->mixed_stage_off + stage_bytes);
+                L->mixed_val_cap = cap32_min; /* the smallest CTA's share (statistics only) */
+                L->mixed_smem_bytes = GSLAM_RES_SMEM_MAX;
             }
-            /* FP64 one-reduction solver: FP64 values | local columns | z of own and halo rows
-             * (32 B each) | u, v of the first `block` halo rows (64 B each); D^-1 stays in
-             * global memory (L2), leaving the shared memory to the values */
-            const int64_t z64_bytes = (32 * p_cap + 127) / 128 * 128;
-            const int64_t stage64_bytes = (64 * (int64_t)std::min(h_max, block) + 127) / 128 * 128;
-            const int64_t cap_cg = ((int64_t)GSLAM_RES_SMEM_MAX - col_bytes - z64_bytes - stage64_bytes) / 8 / 288 * 288;
-            if (cap_cg >= 0) {
+            if (fit64) {
                 L->cg_ok = true;
-                L->cg_val_cap = std::min<int64_t>(cap_cg, 9 * max_slots);
-                L->cg_halo_off = 8 * L->cg_val_cap + col_bytes;
-                L->cg_stage_off = L->cg_halo_off + z64_bytes;
-                L->cg_smem_bytes = (size_t)(L->cg_stage_off + stage64_bytes);
+                L->cg_val_cap = cap64_min;
+                L->cg_smem_bytes = GSLAM_RES_SMEM_MAX;
             }
             if (L->resident || L->mixed_ok || L->cg_ok) {
                 CK(dupload(m, st, &L->lcol, lcol));
@@ -393,15 +385,12 @@ static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts 
         }
     }
     P.cta_slice = L->cta_slice;
-    P.smem_val_cap = mixed ? L->mixed_val_cap : cg ? L->cg_val_cap : L->smem_val_cap;
-    P.smem_dinv_off = L->mixed_dinv_off;
-    P.smem_halo_off = cg ? L->cg_halo_off : L->mixed_halo_off;
-    P.smem_stage_off = cg ? L->cg_stage_off : L->mixed_stage_off;
+    P.smem_val_cap = L->smem_val_cap;
+    P.smem_budget = mixed ? (int64_t)L->mixed_smem_bytes : cg ? (int64_t)L->cg_smem_bytes : (int64_t)L->smem_bytes;
     P.lcol = L->lcol;
     P.halo_ptr = L->halo_ptr;
     P.halo_rows = L->halo_rows;
     P.row_export = L->row_export;
-    P.smem_p_off = L->smem_p_off;
     tr.step("memsets");
     CK(record_event(L->ev0, st));
     if (mixed) CK(launch_pcg_mixed(st, P, grid, L->res_block, L->mixed_smem_bytes, false));

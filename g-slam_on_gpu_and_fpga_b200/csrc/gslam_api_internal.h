@@ -42,19 +42,15 @@ struct DevLayout {
     bool resident = false;
     int res_grid = 0, res_block = 0;
     int *cta_slice = nullptr;      /* [res_grid + 1] */
-    int64_t smem_val_cap = 0;      /* doubles staged per CTA */
+    int64_t smem_val_cap = 0;      /* doubles staged by the CTA that stages fewest */
     int *lcol = nullptr, *halo_ptr = nullptr, *halo_rows = nullptr; /* CTA-local columns, halo lists */
     unsigned char *row_export = nullptr; /* rows some other CTA's halo lists */
-    int64_t smem_p_off = 0;        /* staged p, after values and columns */
     size_t smem_bytes = 0;
     bool mixed_ok = false;          /* the mixed solver's shared-memory layout fits */
-    int64_t mixed_val_cap = 0;     /* floats staged per CTA */
-    int64_t mixed_dinv_off = 0, mixed_halo_off = 0;
-    int64_t mixed_stage_off = 0;     /* halo u, v staging (cp.async) */
-    size_t mixed_smem_bytes = 0;
+    int64_t mixed_val_cap = 0;     /* floats staged by the CTA that stages fewest */
+    size_t mixed_smem_bytes = 0;   /* dynamic shared memory per CTA (each CTA's layout: mixed_smem_layout) */
     bool cg_ok = false;             /* the FP64 one-reduction solver's layout fits */
-    int64_t cg_val_cap = 0;        /* doubles staged per CTA */
-    int64_t cg_halo_off = 0, cg_stage_off = 0;
+    int64_t cg_val_cap = 0;        /* doubles staged by the CTA that stages fewest */
     size_t cg_smem_bytes = 0;
     double *w4 = nullptr;          /* its sixth published vector (made on first use) */
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;   /* brackets the solver launch */

@@ -78,16 +78,60 @@ struct PcgParams {
     long long spin_limit;  /* clock cycles a barrier may wait */
     int absent_cta;        /* test hook: CTA that leaves before its first barrier, -1 = none */
     const int *cta_slice;  /* resident solver: [grid + 1] first slice of each CTA */
-    int64_t smem_val_cap;  /* resident solver: values (multiple of 288) staged in shared memory */
-    int64_t smem_dinv_off; /* mixed solver: byte offsets of own-row D^-1 and of z (own + halo rows) */
-    int64_t smem_halo_off;
-    int64_t smem_stage_off; /* mixed solver: halo rows' u, v (32 B per row), copied in with cp.async */
+    int64_t smem_val_cap;  /* resident solvers: the smallest CTA's staged values (statistics only) */
     const int *lcol;       /* resident solver: per slot, CTA-local column index (own rows, then halo) */
     const int *halo_ptr;   /* resident solver: [grid + 1] halo list bounds per CTA */
     const int *halo_rows;  /* resident solver: halo rows (new row indices) */
     const unsigned char *row_export; /* 1 for rows in another CTA's halo: only those are published */
-    int64_t smem_p_off;    /* resident solver: byte offset of the staged p (32 B per row) */
+    int64_t smem_budget;   /* resident, mixed and FP64 one-reduction solvers: dynamic shared memory per CTA */
 };
+
+/* Shared-memory layout of one CTA of the FP64 resident solver, from its own sizes: local
+ * columns and p of own and halo rows (32 B each) after the values, and as many values (whole
+ * multiples of 288) as the budget leaves (val_cap < 0: the fixed parts alone do not fit). */
+struct ResidentSmem {
+    int64_t val_cap, col_off, p_off, end;
+};
+__host__ __device__ inline ResidentSmem resident_smem_layout(int64_t n_slots, int64_t n_slices, int64_t n_halo,
+                                                             int64_t budget) {
+    auto up = [](int64_t b) { return (b + 127) / 128 * 128; };
+    const int64_t col_b = up(4 * n_slots), p_b = 32 * (32 * n_slices + n_halo);
+    ResidentSmem m;
+    const int64_t fixed = col_b + p_b;
+    m.val_cap = budget >= fixed ? (budget - fixed) / 8 / 288 * 288 : -1;
+    const int64_t nv = m.val_cap > 9 * n_slots ? 9 * n_slots : m.val_cap;
+    m.col_off = up(8 * (nv > 0 ? nv : 0));
+    m.p_off = m.col_off + col_b;
+    m.end = m.p_off + p_b;
+    return m;
+}
+
+/* Shared-memory layout of one CTA of the mixed / FP64 one-reduction solver, from its own
+ * sizes: the fixed parts (local columns, D^-1 of own rows when staged, z of own and halo
+ * rows, the halo's u and v for the first `block` halo rows) after the values, and as many
+ * values (whole multiples of 288, one block position of a slice) as the budget leaves.
+ * val_cap < 0: the fixed parts alone exceed the budget. */
+struct MixedSmem {
+    int64_t val_cap, col_off, dinv_off, halo_off, stage_off, end;
+};
+__host__ __device__ inline MixedSmem mixed_smem_layout(int64_t elem, bool fp64, int64_t n_slots, int64_t n_slices,
+                                                       int64_t n_halo, int64_t block, int64_t budget) {
+    auto up = [](int64_t b) { return (b + 127) / 128 * 128; };
+    const int64_t col_b = up(4 * n_slots);
+    const int64_t dinv_b = fp64 ? 0 : 2304 * n_slices;
+    const int64_t z_b = up(4 * elem * (32 * n_slices + n_halo));
+    const int64_t stage_b = up(8 * elem * (n_halo < block ? n_halo : block));
+    MixedSmem m;
+    const int64_t fixed = col_b + dinv_b + z_b + stage_b;
+    m.val_cap = budget >= fixed ? (budget - fixed) / elem / 288 * 288 : -1;
+    const int64_t nv = m.val_cap > 9 * n_slots ? 9 * n_slots : m.val_cap;
+    m.col_off = up(elem * (nv > 0 ? nv : 0));
+    m.dinv_off = m.col_off + col_b;
+    m.halo_off = m.dinv_off + dinv_b;
+    m.stage_off = m.halo_off + z_b;
+    m.end = m.stage_off + stage_b;
+    return m;
+}
 
 /* Round cost terms per edge and their total (kernels.cu); block_sums holds
  * edge_cost_blocks(n_edges) doubles. */

@@ -180,15 +180,18 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     const int row0 = 32 * s0, n_loc = 32 * (s1 - s0);
     const int64_t slot0 = __ldg(P.slice_ptr + s0), slot1 = __ldg(P.slice_ptr + s1);
     const int64_t nval = 9 * (slot1 - slot0);
-    const int64_t nsm = nval < P.smem_val_cap ? nval : P.smem_val_cap;
     const int h0 = __ldg(P.halo_ptr + blockIdx.x), h1 = __ldg(P.halo_ptr + blockIdx.x + 1);
-    /* dynamic shared memory: T values | local columns | D^-1 of own rows (FP32 only) |
-     * z of own + halo rows | halo u, v (8 T per row) */
+    /* dynamic shared memory, laid out per CTA from its own sizes (mixed_smem_layout, the
+     * host's feasibility check uses the same function): T values as far as they fit |
+     * local columns | D^-1 of own rows (FP32 only) | z of own + halo rows | halo u, v
+     * (8 T per row, the first BS halo rows) */
+    const MixedSmem ml = mixed_smem_layout(sizeof(T), F64, slot1 - slot0, s1 - s0, h1 - h0, BS, P.smem_budget);
+    const int64_t nsm = nval < ml.val_cap ? nval : ml.val_cap;
     T *sval = reinterpret_cast<T *>(smem);
-    int *scol = reinterpret_cast<int *>(smem + sizeof(T) * P.smem_val_cap);
-    double *sdinv = reinterpret_cast<double *>(smem + P.smem_dinv_off);
-    T *sz = reinterpret_cast<T *>(smem + P.smem_halo_off);
-    T *sstage = reinterpret_cast<T *>(smem + P.smem_stage_off);
+    int *scol = reinterpret_cast<int *>(smem + ml.col_off);
+    double *sdinv = reinterpret_cast<double *>(smem + ml.dinv_off);
+    T *sz = reinterpret_cast<T *>(smem + ml.halo_off);
+    T *sstage = reinterpret_cast<T *>(smem + ml.stage_off);
 
     if (threadIdx.x == 0) {
         tma_mbar_init(&s_bar, 1);

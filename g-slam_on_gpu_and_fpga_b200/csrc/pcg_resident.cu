@@ -55,12 +55,15 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     const int s0 = __ldg(P.cta_slice + blockIdx.x), s1 = __ldg(P.cta_slice + blockIdx.x + 1);
     const int64_t slot0 = __ldg(P.slice_ptr + s0), slot1 = __ldg(P.slice_ptr + s1);
     const int64_t nval = 9 * (slot1 - slot0);
-    const int64_t nsm = nval < P.smem_val_cap ? nval : P.smem_val_cap; /* multiple of 288 */
-    double *sval = reinterpret_cast<double *>(smem);
-    int *scol = reinterpret_cast<int *>(smem + 8 * P.smem_val_cap);   /* local column indices */
-    double *sp = reinterpret_cast<double *>(smem + P.smem_p_off);     /* p of own + halo rows */
     const int n_loc = 32 * (s1 - s0), row0 = 32 * s0;
     const int h0 = __ldg(P.halo_ptr + blockIdx.x), h1 = __ldg(P.halo_ptr + blockIdx.x + 1);
+    /* this CTA's own layout (resident_smem_layout; the host checked that it fits): values as
+     * far as they fit | local column indices | p of own + halo rows */
+    const ResidentSmem ml = resident_smem_layout(slot1 - slot0, s1 - s0, h1 - h0, P.smem_budget);
+    const int64_t nsm = nval < ml.val_cap ? nval : ml.val_cap; /* multiple of 288 */
+    double *sval = reinterpret_cast<double *>(smem);
+    int *scol = reinterpret_cast<int *>(smem + ml.col_off);
+    double *sp = reinterpret_cast<double *>(smem + ml.p_off);
 
     /* ---- stage this CTA's matrix share ---- */
     if (threadIdx.x == 0) {
