@@ -213,7 +213,9 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             CK(dupload(m, st, &L->cta_slice, cs));
             L->partial_capacity = std::max(L->partial_capacity, rgrid);
             /* CTA-local column indices (own rows first, then the CTA's halo) and halo lists */
-            std::vector<int> lcol(S.n_slots, 0), hptr(rgrid + 1, 0), hrows;
+            std::vector<unsigned short> lcol(S.n_slots, 0);
+            std::vector<int> hptr(rgrid + 1, 0), hrows;
+            bool cols16 = true; /* every CTA's own + halo rows fit 16-bit local indices */
             /* mixed / FP64 one-reduction solvers: every CTA's own layout must fit */
             bool fit32 = true, fit64 = true, fit_res = true;
             int64_t cap32_min = INT64_MAX, cap64_min = INT64_MAX, cap_res_min = INT64_MAX;
@@ -227,11 +229,13 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 }
                 std::sort(rem.begin(), rem.end());
                 rem.erase(std::unique(rem.begin(), rem.end()), rem.end());
+                if (nloc + (int64_t)rem.size() > 65535) cols16 = false;
                 for (int64_t t = a0; t < a1; t++) {
                     const int c = S.col[t];
-                    if (c < 0) lcol[t] = 0;
-                    else if (c >= row0 && c < row1) lcol[t] = c - row0;
-                    else lcol[t] = nloc + (int)(std::lower_bound(rem.begin(), rem.end(), c) - rem.begin());
+                    int lc = 0;
+                    if (c >= row0 && c < row1) lc = c - row0;
+                    else if (c >= 0) lc = nloc + (int)(std::lower_bound(rem.begin(), rem.end(), c) - rem.begin());
+                    lcol[t] = (unsigned short)lc;
                 }
                 hptr[i + 1] = hptr[i] + (int)rem.size();
                 hrows.insert(hrows.end(), rem.begin(), rem.end());
@@ -250,6 +254,7 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             }
             /* FP64: values | local columns | staged p (32 B per own or halo row), each CTA's
              * from its own sizes (resident_smem_layout) */
+            if (!cols16) fit_res = fit32 = fit64 = false;
             if (fit_res && !o.disable_resident) {
                 L->resident = true;
                 L->smem_val_cap = cap_res_min; /* the smallest CTA's share (statistics only) */

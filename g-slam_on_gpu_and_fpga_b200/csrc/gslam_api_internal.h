@@ -43,7 +43,8 @@ struct DevLayout {
     int res_grid = 0, res_block = 0;
     int *cta_slice = nullptr;      /* [res_grid + 1] */
     int64_t smem_val_cap = 0;      /* doubles staged by the CTA that stages fewest */
-    int *lcol = nullptr, *halo_ptr = nullptr, *halo_rows = nullptr; /* CTA-local columns, halo lists */
+    unsigned short *lcol = nullptr;  /* CTA-local 16-bit columns */
+    int *halo_ptr = nullptr, *halo_rows = nullptr; /* halo lists */
     unsigned char *row_export = nullptr; /* rows some other CTA's halo lists */
     size_t smem_bytes = 0;
     bool mixed_ok = false;          /* the mixed solver's shared-memory layout fits */
