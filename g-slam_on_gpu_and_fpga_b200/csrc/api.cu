@@ -213,12 +213,14 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             CK(dupload(m, st, &L->cta_slice, cs));
             L->partial_capacity = std::max(L->partial_capacity, rgrid);
             /* CTA-local column indices (own rows first, then the CTA's halo) and halo lists */
-            std::vector<unsigned short> lcol(S.n_slots, 0);
-            std::vector<int> hptr(rgrid + 1, 0), hrows;
-            bool cols16 = true; /* every CTA's own + halo rows fit 16-bit local indices */
+            std::vector<int> lcol(S.n_slots, 0), hptr(rgrid + 1, 0), hrows;
             /* mixed / FP64 one-reduction solvers: every CTA's own layout must fit */
             bool fit32 = true, fit64 = true, fit_res = true;
             int64_t cap32_min = INT64_MAX, cap64_min = INT64_MAX, cap_res_min = INT64_MAX;
+            /* the largest CTA's layout end: the launch asks for no more shared memory than
+             * that (shared memory and L1 share the SM's SRAM, and these kernels read D^-1 and
+             * row data through L1) */
+            int64_t end32 = 0, end64 = 0, end_res = 0;
             for (int i = 0; i < rgrid; i++) {
                 const int row0 = 32 * cs[i], row1 = 32 * cs[i + 1], nloc = row1 - row0;
                 const int64_t a0 = S.slice_ptr[cs[i]], a1 = S.slice_ptr[cs[i + 1]];
@@ -229,13 +231,11 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 }
                 std::sort(rem.begin(), rem.end());
                 rem.erase(std::unique(rem.begin(), rem.end()), rem.end());
-                if (nloc + (int64_t)rem.size() > 65535) cols16 = false;
                 for (int64_t t = a0; t < a1; t++) {
                     const int c = S.col[t];
-                    int lc = 0;
-                    if (c >= row0 && c < row1) lc = c - row0;
-                    else if (c >= 0) lc = nloc + (int)(std::lower_bound(rem.begin(), rem.end(), c) - rem.begin());
-                    lcol[t] = (unsigned short)lc;
+                    if (c < 0) lcol[t] = 0;
+                    else if (c >= row0 && c < row1) lcol[t] = c - row0;
+                    else lcol[t] = nloc + (int)(std::lower_bound(rem.begin(), rem.end(), c) - rem.begin());
                 }
                 hptr[i + 1] = hptr[i] + (int)rem.size();
                 hrows.insert(hrows.end(), rem.begin(), rem.end());
@@ -249,16 +249,18 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
                 cap_res_min = std::min(cap_res_min, std::min<int64_t>(lr.val_cap, 9 * (a1 - a0)));
                 fit32 = fit32 && l32.val_cap >= 0;
                 fit64 = fit64 && l64.val_cap >= 0;
+                end_res = std::max(end_res, lr.end);
+                end32 = std::max(end32, l32.end);
+                end64 = std::max(end64, l64.end);
                 cap32_min = std::min(cap32_min, std::min<int64_t>(l32.val_cap, 9 * (a1 - a0)));
                 cap64_min = std::min(cap64_min, std::min<int64_t>(l64.val_cap, 9 * (a1 - a0)));
             }
             /* FP64: values | local columns | staged p (32 B per own or halo row), each CTA's
              * from its own sizes (resident_smem_layout) */
-            if (!cols16) fit_res = fit32 = fit64 = false;
             if (fit_res && !o.disable_resident) {
                 L->resident = true;
                 L->smem_val_cap = cap_res_min; /* the smallest CTA's share (statistics only) */
-                L->smem_bytes = GSLAM_RES_SMEM_MAX;
+                L->smem_bytes = (size_t)end_res;
             }
             /* mixed: FP32 values | local columns | D^-1 of own rows (2304 B per slice) | z of
              * own and halo rows (16 B each) | u, v of the first `block` halo rows (32 B each,
@@ -269,12 +271,12 @@ int gslam_layout_upload(DevLayout *L, const gslam_structure &S, cudaStream_t st,
             if (fit32) {
                 L->mixed_ok = true;
                 L->mixed_val_cap = cap32_min; /* the smallest CTA's share (statistics only) */
-                L->mixed_smem_bytes = GSLAM_RES_SMEM_MAX;
+                L->mixed_smem_bytes = (size_t)end32;
             }
             if (fit64) {
                 L->cg_ok = true;
                 L->cg_val_cap = cap64_min;
-                L->cg_smem_bytes = GSLAM_RES_SMEM_MAX;
+                L->cg_smem_bytes = (size_t)end64;
             }
             if (L->resident || L->mixed_ok || L->cg_ok) {
                 CK(dupload(m, st, &L->lcol, lcol));
@@ -391,7 +393,9 @@ static int layout_solve_enqueue(DevLayout *L, cudaStream_t st, const gslam_opts 
     }
     P.cta_slice = L->cta_slice;
     P.smem_val_cap = L->smem_val_cap;
-    P.smem_budget = mixed ? (int64_t)L->mixed_smem_bytes : cg ? (int64_t)L->cg_smem_bytes : (int64_t)L->smem_bytes;
+    /* every CTA lays its share out against the full budget, as the host's check did; the
+     * launch asks for the largest resulting layout */
+    P.smem_budget = GSLAM_RES_SMEM_MAX;
     P.lcol = L->lcol;
     P.halo_ptr = L->halo_ptr;
     P.halo_rows = L->halo_rows;

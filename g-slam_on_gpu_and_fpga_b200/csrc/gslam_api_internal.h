@@ -43,13 +43,12 @@ struct DevLayout {
     int res_grid = 0, res_block = 0;
     int *cta_slice = nullptr;      /* [res_grid + 1] */
     int64_t smem_val_cap = 0;      /* doubles staged by the CTA that stages fewest */
-    unsigned short *lcol = nullptr;  /* CTA-local 16-bit columns */
-    int *halo_ptr = nullptr, *halo_rows = nullptr; /* halo lists */
+    int *lcol = nullptr, *halo_ptr = nullptr, *halo_rows = nullptr; /* CTA-local columns, halo lists */
     unsigned char *row_export = nullptr; /* rows some other CTA's halo lists */
     size_t smem_bytes = 0;
     bool mixed_ok = false;          /* the mixed solver's shared-memory layout fits */
     int64_t mixed_val_cap = 0;     /* floats staged by the CTA that stages fewest */
-    size_t mixed_smem_bytes = 0;   /* dynamic shared memory per CTA (each CTA's layout: mixed_smem_layout) */
+    size_t mixed_smem_bytes = 0;   /* dynamic shared memory per launch: the largest CTA layout (mixed_smem_layout) */
     bool cg_ok = false;             /* the FP64 one-reduction solver's layout fits */
     int64_t cg_val_cap = 0;        /* doubles staged by the CTA that stages fewest */
     size_t cg_smem_bytes = 0;

@@ -79,15 +79,15 @@ struct PcgParams {
     int absent_cta;        /* test hook: CTA that leaves before its first barrier, -1 = none */
     const int *cta_slice;  /* resident solver: [grid + 1] first slice of each CTA */
     int64_t smem_val_cap;  /* resident solvers: the smallest CTA's staged values (statistics only) */
-    const unsigned short *lcol; /* resident solvers: per slot, CTA-local column index (own rows, then halo) */
+    const int *lcol;       /* resident solver: per slot, CTA-local column index (own rows, then halo) */
     const int *halo_ptr;   /* resident solver: [grid + 1] halo list bounds per CTA */
     const int *halo_rows;  /* resident solver: halo rows (new row indices) */
     const unsigned char *row_export; /* 1 for rows in another CTA's halo: only those are published */
     int64_t smem_budget;   /* resident, mixed and FP64 one-reduction solvers: dynamic shared memory per CTA */
 };
 
-/* Shared-memory layout of one CTA of the FP64 resident solver, from its own sizes: 16-bit
- * local columns and p of own and halo rows (32 B each) after the values, and as many values (whole
+/* Shared-memory layout of one CTA of the FP64 resident solver, from its own sizes: local
+ * columns and p of own and halo rows (32 B each) after the values, and as many values (whole
  * multiples of 288) as the budget leaves (val_cap < 0: the fixed parts alone do not fit). */
 struct ResidentSmem {
     int64_t val_cap, col_off, p_off, end;
@@ -95,7 +95,7 @@ struct ResidentSmem {
 __host__ __device__ inline ResidentSmem resident_smem_layout(int64_t n_slots, int64_t n_slices, int64_t n_halo,
                                                              int64_t budget) {
     auto up = [](int64_t b) { return (b + 127) / 128 * 128; };
-    const int64_t col_b = up(2 * n_slots), p_b = 32 * (32 * n_slices + n_halo);
+    const int64_t col_b = up(4 * n_slots), p_b = 32 * (32 * n_slices + n_halo);
     ResidentSmem m;
     const int64_t fixed = col_b + p_b;
     m.val_cap = budget >= fixed ? (budget - fixed) / 8 / 288 * 288 : -1;
@@ -107,7 +107,7 @@ __host__ __device__ inline ResidentSmem resident_smem_layout(int64_t n_slots, in
 }
 
 /* Shared-memory layout of one CTA of the mixed / FP64 one-reduction solver, from its own
- * sizes: the fixed parts (16-bit local columns, D^-1 of own rows when staged, z of own and halo
+ * sizes: the fixed parts (local columns, D^-1 of own rows when staged, z of own and halo
  * rows, the halo's u and v for the first `block` halo rows) after the values, and as many
  * values (whole multiples of 288, one block position of a slice) as the budget leaves.
  * val_cap < 0: the fixed parts alone exceed the budget. */
@@ -117,7 +117,7 @@ struct MixedSmem {
 __host__ __device__ inline MixedSmem mixed_smem_layout(int64_t elem, bool fp64, int64_t n_slots, int64_t n_slices,
                                                        int64_t n_halo, int64_t block, int64_t budget) {
     auto up = [](int64_t b) { return (b + 127) / 128 * 128; };
-    const int64_t col_b = up(2 * n_slots);
+    const int64_t col_b = up(4 * n_slots);
     const int64_t dinv_b = fp64 ? 0 : 2304 * n_slices;
     const int64_t z_b = up(4 * elem * (32 * n_slices + n_halo));
     const int64_t stage_b = up(8 * elem * (n_halo < block ? n_halo : block));

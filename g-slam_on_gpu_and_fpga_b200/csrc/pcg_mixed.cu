@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     const MixedSmem ml = mixed_smem_layout(sizeof(T), F64, slot1 - slot0, s1 - s0, h1 - h0, BS, P.smem_budget);
     const int64_t nsm = nval < ml.val_cap ? nval : ml.val_cap;
     T *sval = reinterpret_cast<T *>(smem);
-    unsigned short *scol = reinterpret_cast<unsigned short *>(smem + ml.col_off); /* 16-bit local columns */
+    int *scol = reinterpret_cast<int *>(smem + ml.col_off);
     double *sdinv = reinterpret_cast<double *>(smem + ml.dinv_off);
     T *sz = reinterpret_cast<T *>(smem + ml.halo_off);
     T *sstage = reinterpret_cast<T *>(smem + ml.stage_off);
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned vbytes = (unsigned)(sizeof(T) * nsm), cbytes = (unsigned)(2 * (slot1 - slot0));
+        const unsigned vbytes = (unsigned)(sizeof(T) * nsm), cbytes = (unsigned)(4 * (slot1 - slot0));
         const unsigned dbytes = F64 ? 0u : (unsigned)(2304 * (s1 - s0));
         tma_mbar_expect_tx(&s_bar, vbytes + cbytes + dbytes);
         if (vbytes) tma_bulk_g2s(sval, Inner<T>::val(P) + 9 * slot0, vbytes, &s_bar);
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg_mixed(PcgParams P) {
             double part[3] = { 0.0, 0.0, 0.0 };
             T q0 = (T)0, q1 = (T)0, q2 = (T)0;
             if (mine) {
-                const unsigned short *cb = scol + lslot + lane;
+                const int *cb = scol + lslot + lane;
                 const int jend = len;
                 const int jsm = j_sm;
                 int j = 0;

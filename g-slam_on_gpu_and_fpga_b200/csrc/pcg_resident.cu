@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     const ResidentSmem ml = resident_smem_layout(slot1 - slot0, s1 - s0, h1 - h0, P.smem_budget);
     const int64_t nsm = nval < ml.val_cap ? nval : ml.val_cap; /* multiple of 288 */
     double *sval = reinterpret_cast<double *>(smem);
-    unsigned short *scol = reinterpret_cast<unsigned short *>(smem + ml.col_off); /* 16-bit local columns */
+    int *scol = reinterpret_cast<int *>(smem + ml.col_off);
     double *sp = reinterpret_cast<double *>(smem + ml.p_off);
 
     /* ---- stage this CTA's matrix share ---- */
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned vbytes = (unsigned)(8 * nsm), cbytes = (unsigned)(2 * (slot1 - slot0));
+        const unsigned vbytes = (unsigned)(8 * nsm), cbytes = (unsigned)(4 * (slot1 - slot0));
         tma_mbar_expect_tx(&s_bar, vbytes + cbytes);
         if (vbytes) tma_bulk_g2s(sval, P.val + 9 * slot0, vbytes, &s_bar);
         if (cbytes) tma_bulk_g2s(scol, P.lcol + slot0, cbytes, &s_bar);
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(BS, 1) k_pcg64_res(PcgParams P) {
     /* how many of the row's blocks have their values in shared memory */
     const int j_sm = min(len, max(0, ((int)nsm - 9 * lslot) / 288));
     const double *gval = P.val + 9 * slot0;  /* global copy of this CTA's share */
-    const unsigned short *cb = scol + lslot + lane;
+    const int *cb = scol + lslot + lane;
 
     /* the halo row whose z and previous p this thread prefetches after each phase-B
      * barrier (rows beyond the CTA's thread count are read in phase A instead) */
