@@ -15,8 +15,9 @@
  * graphs and a graph spans a contiguous range of CTAs. Each iteration has the two
  * grid barriers of the single-graph solver; the dot products are per graph:
  *   every warp reduces each of its slices into a per-slice partial in shared memory;
- *   thread t < (graphs of this CTA) adds its graph's slice partials in slice order
- *   into the CTA's slot of that graph's partial array; after the grid barrier warp t
+ *   thread t < (graphs of this CTA) adds its graph's slice partials in slice order (the
+ *   graph's contiguous slice range, found once per launch) into the CTA's slot of that
+ *   graph's partial array; after the grid barrier warp t
  *   sums the graph's CTA partials in CTA order (lane-strided, shuffle tree) and
  *   lane 0 advances that graph's scalars in shared memory.
  * Every CTA that owns rows of a graph computes the same scalars from the same sums
@@ -188,6 +189,18 @@ __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B)
     const int nlg = ns > 0 ? __ldg(B.cta_g1 + c) - g0 + 1 : 0;
     int epoch = 0;
     if (c == P.absent_cta) return; /* test hook, see pcg.cu */
+    /* thread t < nlg: the range of this CTA's slices that belong to its graph g0 + t (a
+     * graph's slices are contiguous), found once, and its slot in the graph's partials */
+    int my_lo = 0, my_hi = 0, my_slot = 0;
+    if ((int)threadIdx.x < nlg) {
+        const int g = g0 + threadIdx.x;
+        int sl = 0;
+        while (sl < ns && __ldg(B.slice_graph + s0 + sl) < g) sl++;
+        my_lo = sl;
+        while (sl < ns && __ldg(B.slice_graph + s0 + sl) == g) sl++;
+        my_hi = sl;
+        my_slot = __ldg(B.part_off + g) + (c - __ldg(B.graph_cta0 + g));
+    }
 
     /* per-slice partials -> this CTA's slot of each graph's partial array, then the
      * grid barrier, then the graph totals into tot[v][t] (shared) */
@@ -195,16 +208,13 @@ __global__ void __launch_bounds__(BS, 2) k_pcg_batch(PcgParams P, BatchParams B)
         __syncthreads();
         double *part = B.partials + (size_t)(epoch & 1) * 2 * B.total_parts;
         if ((int)threadIdx.x < nlg) {
-            const int g = g0 + threadIdx.x;
             double a0 = 0.0, a1 = 0.0;
-            for (int sl = 0; sl < ns; sl++) {
-                if (__ldg(B.slice_graph + s0 + sl) != g) continue;
+            for (int sl = my_lo; sl < my_hi; sl++) {
                 a0 = a0 + s_part[2 * sl];
                 a1 = a1 + s_part[2 * sl + 1];
             }
-            const int slot = __ldg(B.part_off + g) + (c - __ldg(B.graph_cta0 + g));
-            part[slot] = a0;
-            if (nv > 1) part[B.total_parts + slot] = a1;
+            part[my_slot] = a0;
+            if (nv > 1) part[B.total_parts + my_slot] = a1;
         }
         epoch++;
         if (!grid_barrier(P.gs, (unsigned)epoch, P.spin_limit, &s_ok)) return false;
