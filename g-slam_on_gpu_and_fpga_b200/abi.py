@@ -36,7 +36,7 @@ EXPORTS = [
     "gslam_run", "gslam_linearise", "gslam_assemble", "gslam_solve", "gslam_update",
     "gslam_get_edge_blocks", "gslam_assemble_from_edges", "gslam_get_csr", "gslam_get_dx",
     "gslam_get_diag_inv", "gslam_spmv", "gslam_spmv_bench", "gslam_spmv_bytes", "gslam_read_log", "gslam_free_log",
-    "gslam_version", "gslam_last_error", "gslam_obs_edge_order", "gslam_csr_pattern",
+    "gslam_version", "gslam_last_error", "gslam_obs_edge_order", "gslam_csr_pattern", "gslam_layout_plan",
     "pcg_solve_sparse", "device_graph_init", "device_graph_update", "device_graph_get_row_ptr",
     "device_graph_get_col_idx", "device_build_diag_inv", "device_pcg_solve", "device_graph_free",
     "gslam_dropin_status", "gslam_pcg_solve_static", "gslam_pcg_static_status", "gslam_set_se2_weights", "gslam_adjoint",
@@ -91,6 +91,12 @@ class LogDesc(C.Structure):
 class CSRMatrix(C.Structure):
     _fields_ = [("row_ptr", C.POINTER(C.c_int)), ("col_idx", C.POINTER(C.c_int)),
                 ("values", C.POINTER(C.c_double)), ("dim", C.c_int), ("nnz", C.c_int)]
+
+
+class LayoutInfo(C.Structure):
+    _fields_ = [("n_rows", C.c_int64), ("n_slices", C.c_int64), ("n_slots", C.c_int64),
+                ("nnzb", C.c_int64), ("csr_nnz", C.c_int64), ("anchor_slot", C.c_int64),
+                ("max_width", C.c_int32), ("bare_anchor", C.c_int32)]
 
 
 class ZRec(C.Structure):
@@ -150,6 +156,9 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.c_uint32), C.c_int64, I64P],
             "gslam_csr_pattern": [C.c_uint32, C.c_int64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                   IP, IP, I64P],
+            "gslam_layout_plan": [C.c_uint32, C.c_int64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                  C.c_int, C.c_uint32, IP, C.c_uint32, IP, C.POINTER(LayoutInfo),
+                                  IP, I64P, IP, I64P, I64P, I64P, I64P, I64P],
             "pcg_solve_sparse": [DP, C.POINTER(CSRMatrix), DP, C.c_uint],
             "device_graph_init": [C.POINTER(ZRec), C.c_uint, C.POINTER(URec), C.c_uint, C.c_uint,
                                   C.c_double, C.c_double, DP, IP],
@@ -206,3 +215,32 @@ def default_opts(**kw) -> Opts:
             raise KeyError(k)
         setattr(o, k, v)
     return o
+
+
+def layout_plan(n_poses: int, t1, t2, sell_window: int = 0, segments=None, diag_rows=None) -> dict:
+    """The device layout of an edge list, computed on the host (gslam_layout_plan):
+    sizes plus perm, slice_ptr, col, ctr_ptr, ctr, xi_ptr, xi_ctr, slot_csr as arrays."""
+    L = lib()
+    t1 = np.ascontiguousarray(t1, np.uint32)
+    t2 = np.ascontiguousarray(t2, np.uint32)
+    seg = None if segments is None else np.ascontiguousarray(segments, np.int32)
+    dia = None if diag_rows is None else np.ascontiguousarray(diag_rows, np.int32)
+    head = (C.c_uint32(n_poses), C.c_int64(len(t1)), ptr(t1, C.c_uint32), ptr(t2, C.c_uint32),
+            C.c_int(sell_window), C.c_uint32(0 if seg is None else len(seg)),
+            None if seg is None else ptr(seg, C.c_int), C.c_uint32(0 if dia is None else len(dia)),
+            None if dia is None else ptr(dia, C.c_int))
+    info = LayoutInfo()
+    check(L.gslam_layout_plan(*head, C.byref(info), *([None] * 8)))
+    E = len(t1)
+    out = {k: getattr(info, k) for k, _ in LayoutInfo._fields_}
+    arrays = [("perm", info.n_rows, np.int32), ("slice_ptr", info.n_slices + 1, np.int64),
+              ("col", info.n_slots, np.int32), ("ctr_ptr", info.n_slots + 1, np.int64),
+              ("ctr", 4 * E, np.int64), ("xi_ptr", info.n_rows + 1, np.int64),
+              ("xi_ctr", 2 * E, np.int64), ("slot_csr", info.n_slots, np.int64)]
+    bufs = [np.zeros(max(n, 1), t) for _, n, t in arrays]
+    ct = {np.int32: C.c_int, np.int64: C.c_int64}
+    check(L.gslam_layout_plan(*head, C.byref(info),
+                              *[ptr(b, ct[t]) for b, (_, _, t) in zip(bufs, arrays)]))
+    for (name, n, _), b in zip(arrays, bufs):
+        out[name] = b[:n]
+    return out

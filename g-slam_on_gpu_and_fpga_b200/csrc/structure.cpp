@@ -350,3 +350,51 @@ extern "C" int gslam_csr_pattern(uint32_t n_poses, int64_t n_edges, const uint32
     if (col_idx) memcpy(col_idx, s.csr_col.data(), s.csr_col.size() * sizeof(int));
     return GSLAM_OK;
 }
+
+extern "C" int gslam_layout_plan(uint32_t n_poses, int64_t n_edges, const uint32_t *t1,
+                                 const uint32_t *t2, int sell_window, uint32_t n_segments,
+                                 const int32_t *segment_starts, uint32_t n_diag_rows,
+                                 const int32_t *diag_rows, gslam_layout_info *info, int32_t *perm,
+                                 int64_t *slice_ptr, int32_t *col, int64_t *ctr_ptr, int64_t *ctr,
+                                 int64_t *xi_ptr, int64_t *xi_ctr, int64_t *slot_csr) {
+    if (n_poses == 0 || n_poses > 0x3fffffffu || !info || n_edges < 0 || (n_edges && (!t1 || !t2)) ||
+        (n_segments && !segment_starts) || (n_diag_rows && !diag_rows))
+        return GSLAM_ERR_BAD_INPUT;
+    std::vector<int> segs, diag;
+    if (n_segments) {
+        /* ascending starts inside the rows, the first at row 0 (a batch's graph ranges) */
+        for (uint32_t q = 0; q < n_segments; q++) {
+            const int32_t a = segment_starts[q];
+            if (a < 0 || a >= (int32_t)n_poses || (q == 0 ? a != 0 : a <= segment_starts[q - 1]))
+                return GSLAM_ERR_BAD_INPUT;
+            segs.push_back(a);
+        }
+    }
+    diag.assign(diag_rows, diag_rows + n_diag_rows);
+    gslam_structure s;
+    /* the window the graph constructors use (common_setup in api.cu) */
+    const int window = sell_window <= 0 ? 1024 : sell_window;
+    int rc = gslam_build_structure_ex((int)n_poses, n_edges, t1, t2, window, n_diag_rows ? &diag : nullptr,
+                                      n_segments ? &segs : nullptr, &s);
+    if (rc != GSLAM_OK) return rc;
+    info->n_rows = s.n_rows;
+    info->n_slices = s.n_slices;
+    info->n_slots = s.n_slots;
+    info->nnzb = s.nnzb;
+    info->csr_nnz = (int64_t)s.csr_col.size();
+    info->anchor_slot = s.anchor_slot;
+    info->max_width = s.max_width;
+    info->bare_anchor = s.bare_anchor ? 1 : 0;
+    auto out = [](auto *dst, const auto &v) {
+        if (dst) std::copy(v.begin(), v.end(), dst);
+    };
+    out(perm, s.perm);
+    out(slice_ptr, s.slice_ptr);
+    out(col, s.col);
+    out(ctr_ptr, s.ctr_ptr);
+    out(ctr, s.ctr);
+    out(xi_ptr, s.xi_ptr);
+    out(xi_ctr, s.xi_ctr);
+    out(slot_csr, s.slot_csr);
+    return GSLAM_OK;
+}

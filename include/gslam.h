@@ -201,6 +201,33 @@ int gslam_obs_edge_order(uint32_t n_obs, const uint32_t *obs_landmark, uint32_t 
  * n_poses poses plus the anchor on pose 0. Call with col_idx NULL to get *nnz. */
 int gslam_csr_pattern(uint32_t n_poses, int64_t n_edges, const uint32_t *t1, const uint32_t *t2,
                       int *row_ptr, int *col_idx, int64_t *nnz);
+/*
+ * The sliced 3x3-block layout that gslam_create_* uploads for the edges (t1[e], t2[e])
+ * between n_poses poses, computed on the host (no counterpart in the reference: it
+ * exposes where every block and every edge contribution lands, for tools and tests).
+ * sell_window <= 0 takes the library default (1024), 1 skips the row-length sort.
+ * segment_starts (n_segments ascending rows, the first 0) marks a batch's graphs: rows
+ * keep their order inside their graph's range and the sort windows restart at every
+ * start; with n_segments 0 the rows of the one graph are put in Cuthill-McKee order
+ * first. diag_rows adds a diagonal block to rows that no edge touches (a batch's padding
+ * rows). Every output pointer may be NULL; sizes come back in *info:
+ *   perm[n_rows]                          new row -> pose
+ *   slice_ptr[n_slices + 1]               first slot of each 32-row slice
+ *   col[n_slots]                          new row of each slot's block column, -1 padding
+ *   ctr_ptr[n_slots + 1], ctr[4 n_edges]  per slot, 4 e + sub (0..3 = UL UR BL BR) in edge order
+ *   xi_ptr[n_rows + 1], xi_ctr[2 n_edges] per new row, 2 e + (0 upper, 1 bottom) in edge order
+ *   slot_csr[n_slots]                     position of the slot's entry (0,0) in the reference's
+ *                                         scalar CSR (-1 padding, -2 the bare pose-0 anchor)
+ */
+typedef struct gslam_layout_info {
+    int64_t n_rows, n_slices, n_slots, nnzb, csr_nnz, anchor_slot;
+    int32_t max_width, bare_anchor;
+} gslam_layout_info;
+int gslam_layout_plan(uint32_t n_poses, int64_t n_edges, const uint32_t *t1, const uint32_t *t2,
+                      int sell_window, uint32_t n_segments, const int32_t *segment_starts,
+                      uint32_t n_diag_rows, const int32_t *diag_rows, gslam_layout_info *info,
+                      int32_t *perm, int64_t *slice_ptr, int32_t *col, int64_t *ctr_ptr, int64_t *ctr,
+                      int64_t *xi_ptr, int64_t *xi_ctr, int64_t *slot_csr);
 
 /* ---- reference log files (src/cpu_pcg_fp64/GSLAM.c:415-493, data/README.md) ---- */
 typedef struct gslam_log {
