@@ -15,7 +15,7 @@ the walk) this arithmetic cannot carry a converged solve:
 An FP32 iteration of the device's resident solver takes about half an FP64 one (5.6
 against 11.4 us at N = 100k), so at converged settings the mixed solver is slower than
 the FP64 one, whatever its kernels do; a 3x speed-up at a 1e-6 pose error would need the
-refined FP32 solve to converge in a fifth of FP64's iterations. These tests pin that
+refined FP32 solve to converge in two thirds of FP64's iterations, not 3.5-4.4 times them. These tests pin that
 measurement, so it can be re-checked on any machine.
 """
 import warnings
