@@ -43,6 +43,7 @@ def lib():
         L.or_csr_nnz.restype = C.c_long
         L.or_norm_glibc.restype = C.c_double
         L.or_norm_cr.restype = C.c_double
+        L.or_position_loss_dd.restype = C.c_double
         _lib = L
     return _lib
 
@@ -254,6 +255,47 @@ def run(g: Graph, lam: float, rounds: int, cr: bool = False, tol: float = 1e-6,
     if n < 0:
         raise ValueError("bad graph")
     return poses, diffs[:n], its[:n]
+
+
+def se2_rhs_dd(p_hi, p_lo, ei, ej, meas, info):
+    """xi = -sum J^T Lambda e at double-double poses, in double-double (se2_dd.c):
+    (xi_hi, xi_lo), each [3N]. info = Lambda's diagonal per edge [E, 3], lambda folded in."""
+    L = lib()
+    p_hi = np.ascontiguousarray(p_hi, np.float64).reshape(-1)
+    p_lo = np.ascontiguousarray(p_lo, np.float64).reshape(-1)
+    ei = np.ascontiguousarray(ei, np.uint32); ej = np.ascontiguousarray(ej, np.uint32)
+    meas = np.ascontiguousarray(meas, np.float64); info = np.ascontiguousarray(info, np.float64)
+    xh = np.zeros(len(p_hi)); xl = np.zeros(len(p_hi))
+    rc = L.or_se2_rhs_dd(C.c_long(len(p_hi) // 3), C.c_long(len(ei)), _p(ei, C.c_uint), _p(ej, C.c_uint),
+                         _p(p_hi, C.c_double), _p(p_lo, C.c_double), _p(meas, C.c_double),
+                         _p(info, C.c_double), _p(xh, C.c_double), _p(xl, C.c_double))
+    if rc != 0:
+        raise ValueError("edge pose index out of range")
+    return xh, xl
+
+
+def dd_add_vec(hi, lo, d):
+    """(hi + lo) += d in place (double-double, renormalised); hi, lo contiguous float64."""
+    d = np.ascontiguousarray(d, np.float64).reshape(-1)
+    lib().or_dd_add_vec(C.c_long(len(d)), _p(hi, C.c_double), _p(lo, C.c_double), _p(d, C.c_double))
+
+
+def position_loss_dd(p_hi, p_lo, target):
+    """sum (x - tx)^2 + (y - ty)^2 over poses, in double-double: (hi, lo)."""
+    p_hi = np.ascontiguousarray(p_hi, np.float64).reshape(-1)
+    p_lo = np.ascontiguousarray(p_lo, np.float64).reshape(-1)
+    target = np.ascontiguousarray(target, np.float64).reshape(-1)
+    lo = C.c_double(0.0)
+    hi = lib().or_position_loss_dd(C.c_long(len(p_hi) // 3), _p(p_hi, C.c_double), _p(p_lo, C.c_double),
+                                   _p(target, C.c_double), C.byref(lo))
+    return hi, lo.value
+
+
+def sincos_dd(x_hi: float, x_lo: float = 0.0):
+    """sin and cos of x_hi + x_lo as (hi, lo) pairs (se2_dd.c)."""
+    v = [C.c_double() for _ in range(4)]
+    lib().or_sincos_dd(C.c_double(x_hi), C.c_double(x_lo), *[C.byref(a) for a in v])
+    return (v[0].value, v[1].value), (v[2].value, v[3].value)
 
 
 def cr_sincos(x: float):

@@ -198,3 +198,40 @@ def chord_solve_sparse(poses0, ei, ej, meas, log_w, lam, lu, anchor=1e6, rounds=
         if np.sqrt(np.mean(dx ** 2)) < tol and r + 1 >= min_rounds:
             break
     return p
+
+
+# ---- double-double fixed points, for finite differences below the FP64 noise floor ----
+
+def chord_solve_dd(oracle, poses0, ei, ej, meas, log_w, lam, lu, rounds=60, tol=1e-28):
+    """chord_solve_sparse with xi evaluated in double-double at double-double poses
+    (oracle/se2_dd.c): the FP64 LU only proposes each correction, the double-double
+    xi decides where the iteration stops, so the fixed point comes out to ~1e-30
+    instead of FP64's noise. Angles are not wrapped (the corrections are tiny; the
+    residual wraps itself). Returns (hi, lo), each [N, 3]."""
+    hi = np.array(poses0, np.float64, copy=True).reshape(-1)
+    lo = np.zeros_like(hi)
+    info = lam * np.exp(log_w)
+    scale = np.max(np.abs(hi))
+    for _ in range(rounds):
+        xh, _ = oracle.se2_rhs_dd(hi, lo, ei, ej, meas, info)
+        dx = lu.solve(xh)
+        oracle.dd_add_vec(hi, lo, dx)
+        if np.max(np.abs(dx)) < tol * scale:
+            break
+    return hi.reshape(-1, 3), lo.reshape(-1, 3)
+
+
+def fd_log_weights_dd(oracle, poses, ei, ej, meas, log_w, lam, lu, target, pairs, h):
+    """Central differences of position_loss(fixed point) in the log weights (edge e,
+    component k) for each pair, with double-double fixed points and loss; the step is
+    the one the FP64 weights actually take (fl(w + h) - w, fl(w - h) - w)."""
+    out = []
+    for e, k in pairs:
+        lp, lm = log_w.copy(), log_w.copy()
+        lp[e, k] += h
+        lm[e, k] -= h
+        step = (lp[e, k] - log_w[e, k]) - (lm[e, k] - log_w[e, k])
+        Lp = oracle.position_loss_dd(*chord_solve_dd(oracle, poses, ei, ej, meas, lp, lam, lu), target)
+        Lm = oracle.position_loss_dd(*chord_solve_dd(oracle, poses, ei, ej, meas, lm, lam, lu), target)
+        out.append(((Lp[0] - Lm[0]) + (Lp[1] - Lm[1])) / step)
+    return np.array(out)
