@@ -89,6 +89,25 @@ def test_adjoint_matches_finite_differences(setup, h, rel):
     assert np.linalg.norm(fd - adj) <= rel * np.linalg.norm(adj), (fd, adj)
 
 
+def test_adjoint_matches_double_double_differences(setup, oracle):
+    """The configured step, h = 1e-6, without the noise floor above: each difference's
+    fixed points come from chord iterations whose xi is evaluated in double-double at
+    double-double poses (oracle/se2_dd.c), restarted at the GPU's converged poses, and the
+    loss is summed in double-double. 32 seeded pairs, bound 1e-5 relative."""
+    import scipy.sparse.linalg as spl
+    cg, g = setup
+    p = converge(g, cg, cg.log_w)
+    _, dL = R.position_loss(p, cg.gt)
+    _, dlw, _, _ = g.adjoint(dL)
+    H, _ = R.system_sparse(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAM, ANCHOR)
+    lu = spl.splu(H.tocsc(), permc_spec="COLAMD")
+    rng = np.random.default_rng(7)
+    pairs = [(int(rng.integers(len(cg.edge_i))), int(rng.integers(3))) for _ in range(32)]
+    fd = R.fd_log_weights_dd(oracle, p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, LAM, lu, cg.gt, pairs, 1e-6)
+    adj = np.array([dlw[e, k] for e, k in pairs])
+    assert np.linalg.norm(fd - adj) <= 1e-5 * np.linalg.norm(adj), (fd, adj)
+
+
 def test_autograd_function(setup, pkg):
     import torch
     autodiff = importlib.import_module("g-slam_on_gpu_and_fpga_b200.autodiff")
