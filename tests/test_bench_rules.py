@@ -62,3 +62,25 @@ def test_timing_is_the_max_over_ranks_gloo():
         p.join(timeout=30)
     assert got == [(0, 2, 15.0), (1, 2, 15.0)]
     assert all(p.exitcode == 0 for p in procs)
+
+
+def test_cpu_rounds_run_the_references_own_pcg(oracle):
+    """The CPU rounds (cpu_baseline and --impl reference) solve with the reference's own
+    compiled pcg_solve_sparse where oracle/_ref holds it, and their poses are bit for bit
+    the oracle's restatement's (which is what the GPU solvers are held to)."""
+    import numpy as np
+    import pytest
+    if bench.reference_pcg() is None:
+        pytest.skip("reference build absent (oracle/_ref)")
+    synth = importlib.import_module("g-slam_on_gpu_and_fpga_b200.synth")
+    cg = synth.city_grid(3000, seed=5, k_closures=3, radius=2.0)
+    poses, _, kind = bench.oracle_rounds(cg, 2)
+    assert kind == "reference"
+    p = cg.init.copy()
+    for _ in range(2):
+        blocks, _ = oracle.se2_linearise(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, bench.LAMBDA)
+        rp, ci, va, xi = oracle.csr_build_anchor(3 * cg.n_poses, cg.edge_i, cg.edge_j, blocks, 1e6)
+        dx, _, _ = oracle.pcg(rp, ci, va, xi, tol=bench.TOL, max_iter=bench.MAX_ITER)
+        p = p + dx.reshape(-1, 3)
+        p[:, 2] = (p[:, 2] + np.pi) % (2 * np.pi) - np.pi
+    assert np.array_equal(poses.view(np.uint64), p.view(np.uint64))
