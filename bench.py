@@ -307,7 +307,8 @@ def oracle_rounds(cg, rounds, tol=TOL, max_iter=MAX_ITER, lam=LAMBDA):
     and the settings are its own (tol 1e-6, 500 iterations), else the oracle's
     restatement (bit-identical); the SE(2) linearisation and the CSR assembly are the
     oracle's (the reference has no SE(2) factor, and its structure step is wrong above
-    21,845 poses). Returns (poses after them, host seconds, "reference" | "port")."""
+    21,845 poses). Returns (poses after them, host seconds, "reference" | "port", seconds
+    per phase: linearisation + assembly, PCG, pose update)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
 
@@ -316,17 +317,26 @@ def oracle_rounds(cg, rounds, tol=TOL, max_iter=MAX_ITER, lam=LAMBDA):
     ref_solve = reference_pcg() if (tol, max_iter) == (1e-6, 500) else None
     poses = cg.init.copy()
     dim = 3 * cg.n_poses
+    phases = {"linearise_assemble_s": 0.0, "pcg_s": 0.0, "update_s": 0.0}
     t0 = time.perf_counter()
     for _ in range(rounds):
+        ta = time.perf_counter()
         blocks, _ = O.se2_linearise(poses, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, lam)
         rp, ci, va, xi = O.csr_build_anchor(dim, cg.edge_i, cg.edge_j, blocks, 1e6)
+        tb = time.perf_counter()
         if ref_solve is not None:
             dx = ref_solve(rp, ci, va, xi)
         else:
             dx, _, _ = O.pcg(rp, ci, va, xi, tol=tol, max_iter=max_iter)
+        tc = time.perf_counter()
         poses = poses + dx.reshape(-1, 3)
         poses[:, 2] = (poses[:, 2] + np.pi) % (2 * np.pi) - np.pi
-    return poses, time.perf_counter() - t0, ("reference" if ref_solve is not None else "port")
+        phases["linearise_assemble_s"] += tb - ta
+        phases["pcg_s"] += tc - tb
+        phases["update_s"] += time.perf_counter() - tc
+    secs = time.perf_counter() - t0
+    phases = {k: round(v, 3) for k, v in phases.items()}
+    return poses, secs, ("reference" if ref_solve is not None else "port"), phases
 
 
 def cpu_model():
@@ -686,11 +696,12 @@ def run_ours(args):
            "mixed_vs_gpu_fp64": pose_err_rel(finals["mixed"], finals["fp64"])}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        p_or, secs, kind = oracle_rounds(cg, args.steps)
+        p_or, secs, kind, phases = oracle_rounds(cg, args.steps)
         err["gpu_fp64_vs_oracle"] = pose_err_rel(finals["fp64"], p_or)
         err["fp64_cg_vs_oracle"] = pose_err_rel(finals["fp64_cg"], p_or)
         err["mixed_vs_oracle"] = pose_err_rel(finals["mixed"], p_or)
         cpu = {"value": round(args.steps / secs, 5), "unit": UNIT, "cores": 1, "kind": kind, "cpu": cpu_model(),
+               "phases": phases,
                "sample": f"the same {args.steps} GN rounds of the N=100000 workload ({secs:.1f} s), whose poses "
                          "are also the accuracy reference; " + CPU_ROUND_NOTE[kind]}
     met = {"fp64": err.get("gpu_fp64_vs_oracle", 0.0) <= POSE_ERR_BAR}
@@ -778,7 +789,7 @@ def run_reference(args):
         return
     cg = workload(seed=1)
     oracle_rounds(cg, args.warmup)
-    poses, secs, kind = oracle_rounds(cg, args.steps)
+    poses, secs, kind, phases = oracle_rounds(cg, args.steps)
     value = args.steps / secs
     line = {
         "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
@@ -789,6 +800,7 @@ def run_reference(args):
                   "N = 100,000 (its 32-bit structure indexing is wrong above 21,845 poses and its dim x dim "
                   "marker needs 90 GB), and pcg_solve_sparse is single-threaded",
         "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": 1, "kind": kind, "cpu": cpu_model(),
+                         "phases": phases,
                          "sample": f"{args.steps} GN rounds of the N=100000 workload"},
         "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -74,8 +74,9 @@ def test_cpu_rounds_run_the_references_own_pcg(oracle):
         pytest.skip("reference build absent (oracle/_ref)")
     synth = importlib.import_module("g-slam_on_gpu_and_fpga_b200.synth")
     cg = synth.city_grid(3000, seed=5, k_closures=3, radius=2.0)
-    poses, _, kind = bench.oracle_rounds(cg, 2)
+    poses, secs, kind, phases = bench.oracle_rounds(cg, 2)
     assert kind == "reference"
+    assert phases["pcg_s"] > 0 and sum(phases.values()) <= secs + 2e-3
     p = cg.init.copy()
     for _ in range(2):
         blocks, _ = oracle.se2_linearise(p, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, bench.LAMBDA)
