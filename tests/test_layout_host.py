@@ -296,3 +296,24 @@ def test_plan_rejects_bad_input():
     with pytest.raises(G.abi.GslamError):
         G.abi.layout_plan(10, t, t, segments=[0, 5, 5])  # strictly ascending
     assert L.gslam_layout_plan(0, 0, None, None, 0, 0, None, 0, None, None, *([None] * 8)) == G.abi.ERR_BAD_INPUT
+
+
+@pytest.mark.parametrize("n,t1,t2", [(1, [], []), (2, [0], [1]), (3, [1], [2]),
+                                     (33, list(range(32)), list(range(1, 33)))],
+                         ids=["one_pose_no_edges", "two_poses", "pose0_untouched", "33_rows_two_slices"])
+def test_small_and_ragged_graphs(oracle, n, t1, t2):
+    """Edge cases of the plan: a single pose with no edge (only the anchor block), a pose 0
+    that no edge touches, a last slice with one row. Random block values: the replay is
+    the same IEEE arithmetic whatever they are."""
+    t1 = np.array(t1, np.uint32)
+    t2 = np.array(t2, np.uint32)
+    P = _plan(n, t1, t2)
+    blocks = np.random.default_rng(n).standard_normal((len(t1), 42))
+    rp, ci, va, xi = oracle.csr_build_anchor(3 * n, t1, t2, blocks, ANCHOR)
+    acc, vals = _assemble(P, blocks, ANCHOR)
+    assert_bitwise(vals, va, "Omega")
+    assert_bitwise(_assemble_xi(P, blocks), xi, "xi")
+    p = np.random.default_rng(2).standard_normal(3 * n)
+    assert_bitwise(_spmv(P, acc, p), oracle.spmv(rp, ci, va, p), "Omega p")
+    assert P["n_slices"] == (n + 31) // 32
+    assert P["bare_anchor"] == int(not any(a == 0 or b == 0 for a, b in zip(t1, t2)))
