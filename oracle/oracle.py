@@ -257,6 +257,48 @@ def run(g: Graph, lam: float, rounds: int, cr: bool = False, tol: float = 1e-6,
     return poses, diffs[:n], its[:n]
 
 
+def norm_glibc(v) -> float:
+    """The reference's norm (MatrixOps.c:4-16: sqrt of pow(v_i, 2.0) summed in order)."""
+    v = np.ascontiguousarray(v, np.float64)
+    return lib().or_norm_glibc(_p(v, C.c_double), len(v))
+
+
+def run_dense_gj(g: Graph, lam: float, max_rounds: int = 200):
+    """The reference's dense Gauss-Jordan program (src/cpu_gj_fp64/GSLAM.c:89-231, use_diff
+    = 1): each round Omega and xi densely (the anchor, then every edge in make_edges order:
+    the CSR assembly's values), Omega^-1 by Gauss-Jordan without pivoting
+    (MatrixOps.c:29-91; the reference program calls its SYCL-parallel twin), dx = Omega^-1 xi
+    summed in index order from 0.0 (dot -> vec_dot), poses += dx; it stops at
+    diff < 0.01 or when the even- or the odd-numbered rounds' diff has not improved for 10
+    of them (GSLAM.c:218-230). Returns (poses, diffs)."""
+    poses = g.x.copy()
+    diffs = []
+    best = [1e30, 1e30]
+    stale = [0, 0]
+    for n in range(max_rounds):
+        t1, t2, ob = linearise(g, poses, lam, cr=False)
+        rp, ci, va, xi = csr_build(g.dim, t1, t2, ob)
+        inv, rc = gj_inverse(dense_from_csr(rp, ci, va))
+        if rc != 0:
+            raise ValueError("zero pivot")
+        dx = np.zeros(g.dim)
+        for j in range(g.dim):          # every row sums its products in column order
+            dx = dx + inv[:, j] * xi[j]
+        poses = poses + dx.reshape(-1, 3)
+        diff = norm_glibc(dx) / np.sqrt(g.dim)
+        diffs.append(diff)
+        if diff < 0.01:
+            break
+        k = n % 2
+        if diff < best[k]:
+            best[k], stale[k] = diff, 0
+        else:
+            stale[k] += 1
+            if stale[k] >= 10:
+                break
+    return poses, np.array(diffs)
+
+
 def se2_rhs_dd(p_hi, p_lo, ei, ej, meas, info):
     """xi = -sum J^T Lambda e at double-double poses, in double-double (se2_dd.c):
     (xi_hi, xi_lo), each [3N]. info = Lambda's diagonal per edge [E, 3], lambda folded in."""

@@ -6,6 +6,11 @@ reference tree:
   ref_vp_pcg_fp64.npz    scripts/_pose_dumps_vp/cpu_pcg_fp64.txt: the reference CPU program's
                          pose dump of `GSLAM 1 1.0 200 1 victoria-park.log.txt` (116 rounds),
                          which the oracle reproduces bit for bit (tests/test_oracle_pin.py)
+  ref_vp100_gj_fp64.npz  data/victoria-park-100.log.txt, parsed, with
+                         scripts/_pose_dumps_vp/cpu_gj_fp64.txt: the reference's dense
+                         Gauss-Jordan program's pose dump on it at lambda 0.06
+                         (scripts/regen_gj_plot.py), which the oracle's dense run matches to
+                         ~1e-7 (the program inverts with a parallel twin of the serial GJ)
 
 Logs are stored as the arrays the reference's read_data yields (parsed here by
 libgslam's gslam_read_log, itself checked against the oracle's parser); the tests
@@ -53,6 +58,12 @@ def main():
     np.savez_compressed(os.path.join(HERE, "ref_vp_pcg_fp64.npz"), steps=dump[:, 0].astype(np.uint32),
                         poses=dump[:, 1:].copy(), rounds=np.int32(116), lam=np.float64(1.0))
     print("wrote ref_vp_pcg_fp64.npz", dump.shape)
+    log = G.read_log(os.path.join(REF, "data", "victoria-park-100.log.txt"))
+    arrs = log_arrays(log)
+    gj = np.loadtxt(os.path.join(REF, "scripts", "_pose_dumps_vp", "cpu_gj_fp64.txt"), ndmin=2)
+    np.savez_compressed(os.path.join(HERE, "ref_vp100_gj_fp64.npz"), **arrs,
+                        dump_steps=gj[:, 0].astype(np.uint32), dump_poses=gj[:, 1:].copy(), lam=np.float64(0.06))
+    print("wrote ref_vp100_gj_fp64.npz", gj.shape)
 
 
 if __name__ == "__main__":

@@ -209,3 +209,32 @@ def test_gn_fixed_point_direct(oracle):
         blocks, _ = oracle.se2_linearise(q, cg.edge_i, cg.edge_j, cg.meas, cg.log_w, 0.1)
         xi_norm.append(np.linalg.norm(oracle.csr_build_anchor(3 * cg.n_poses, cg.edge_i, cg.edge_j, blocks, 1e6)[3]))
     assert xi_norm[1] < 1e-8 * xi_norm[0]
+
+
+def test_dense_gj_run_vs_reference_gj_dump(oracle):
+    """The dense path (north-star item f): the oracle's run of the reference's Gauss-Jordan
+    program (oracle.run_dense_gj: dense Omega, GJ inverse, dx = Omega^-1 xi, the program's
+    stop rules) on victoria-park-100 at lambda 0.06 against the reference's own committed
+    pose dump of that program (tests/golden/ref_vp100_gj_fp64.npz). The program inverts
+    with a parallel twin of the serial GJ, so the poses agree to rounding amplified over
+    the run (1.2e-7 measured after 35 rounds), not bit for bit."""
+    z = np.load(os.path.join(GOLDEN, "ref_vp100_gj_fp64.npz"))
+    g = oracle.Graph(float(z["delta"]), z["u_step"], z["u"], z["x_step"], z["x"], z["z_step"], z["z_lm"], z["z"])
+    assert np.array_equal(z["dump_steps"], g.x_step)
+    poses, diffs = oracle.run_dense_gj(g, float(z["lam"]))
+    err = np.abs(poses - z["dump_poses"]).max()
+    print(f"victoria-park-100, dense GJ, lambda 0.06: {len(diffs)} rounds, max |pose - dump| {err:.2e}")
+    assert err <= 1e-6
+    assert len(diffs) == 35
+
+
+def test_vp100_gj_fixture_matches_reference_files(oracle):
+    """The committed copies of victoria-park-100 and the GJ dump equal the reference's files."""
+    dump = os.path.join(REF_DUMPS, "cpu_gj_fp64.txt")
+    if not os.path.exists(dump):
+        pytest.skip("reference dump not present")
+    z = np.load(os.path.join(GOLDEN, "ref_vp100_gj_fp64.npz"))
+    assert_bitwise(z["dump_poses"], np.loadtxt(dump, ndmin=2)[:, 1:4], "GJ dump")
+    g = oracle.read_log(ref_data("victoria-park-100.log.txt"))
+    for key, ref in (("u", g.u), ("x", g.x), ("z", g.z), ("z_lm", g.z_lm)):
+        assert np.array_equal(np.asarray(z[key]).reshape(np.shape(ref)), ref), key
