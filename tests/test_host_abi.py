@@ -151,3 +151,30 @@ def test_csr_pattern_rejects_bad_edges():
     G = load_pkg()
     with pytest.raises(G.abi.GslamError):
         _pattern(5, [0, 7], [1, 2])
+
+
+def test_cli_usage_and_header_match_the_reference_program(oracle, tmp_path):
+    """The GSLAM program's argument handling and the two lines it prints before the first
+    round (argument echo; delta and record counts, src/cpu_pcg_fp64/GSLAM.c:13-50) are the
+    reference program's, byte for byte; both reject a wrong argument count with their usage
+    line and exit status 1. (Runs one round: on a machine without a GPU our program stops
+    there with an error, which this test does not look at.)"""
+    import subprocess
+    G = load_pkg()
+    ref_exe = os.path.join(ROOT, "oracle", "_ref", "GSLAM")
+    if not os.path.exists(ref_exe):
+        pytest.skip("reference build absent (oracle/_ref)")
+    cg = G.synth.city_grid(120, seed=4)
+    path = str(tmp_path / "walk.txt")
+    G.synth.write_log(path, G.synth.to_reference_log(cg))
+    ours, ref = G.abi.CLI_PATH, ref_exe
+    for args in ([], ["1", "0.1"]):
+        a = subprocess.run([ours, *args], capture_output=True, text=True, timeout=60)
+        b = subprocess.run([ref, *args], capture_output=True, text=True, timeout=60)
+        assert a.returncode == b.returncode == 1
+        assert a.stdout.replace(ours, "GSLAM") == b.stdout.replace(ref, "GSLAM")
+    env = dict(os.environ, POSE_DUMP_FILE=str(tmp_path / "dump.txt"))
+    a = subprocess.run([ours, "1", "0.1", "1", "0", path], capture_output=True, text=True, timeout=300, env=env)
+    b = subprocess.run([ref, "1", "0.1", "1", "0", path], capture_output=True, text=True, timeout=300, env=env)
+    assert a.stdout.splitlines()[:2] == b.stdout.splitlines()[:2]
+    assert a.returncode in (0, 1) and b.returncode == 0
