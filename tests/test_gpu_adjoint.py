@@ -2,8 +2,10 @@
 torch.autograd.Function (autodiff.GNSolve) on an 800-pose city-grid graph.
 
 Checked against (1) the dense FP64 reference of tests/adjoint_ref.py evaluated at the
-GPU's converged poses, and (2) central finite differences (h = 1e-6 on the log
-weights) of the GPU Gauss-Newton solve on 32 seeded random (edge, component) pairs.
+GPU's converged poses, (2) central finite differences (h = 1e-3 and 1e-6 on the log
+weights) of the GPU Gauss-Newton solve on 32 seeded random (edge, component) pairs, and
+(3) central differences at h = 1e-6 whose fixed points are found in double-double on the
+CPU (oracle/se2_dd.c), free of FP64's noise floor; at N = 10,000 as well.
 Loss: sum of squared position differences to the noise-free walk.
 """
 import importlib
