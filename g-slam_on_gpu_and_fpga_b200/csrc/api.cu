@@ -579,6 +579,7 @@ int gslam_create_se2(const gslam_se2_graph *in, const gslam_opts *opts, gslam_gr
     if (!in || !out) BAD("null argument");
     *out = nullptr;
     if (in->n_poses == 0 || !in->poses) BAD("n_poses == 0 or missing poses");
+    if (in->n_poses > 0x3fffffffu) { g_last_error = "too many poses"; return GSLAM_ERR_TOO_LARGE; }
     if (in->n_edges && (!in->edge_i || !in->edge_j || !in->meas || !in->log_w)) BAD("missing edge arrays");
     for (uint32_t e = 0; e < in->n_edges; e++)
         if (in->edge_i[e] >= in->n_poses || in->edge_j[e] >= in->n_poses) BAD("edge pose out of range");

@@ -178,3 +178,48 @@ def test_cli_usage_and_header_match_the_reference_program(oracle, tmp_path):
     b = subprocess.run([ref, "1", "0.1", "1", "0", path], capture_output=True, text=True, timeout=300, env=env)
     assert a.stdout.splitlines()[:2] == b.stdout.splitlines()[:2]
     assert a.returncode in (0, 1) and b.returncode == 0
+
+
+def test_entry_points_validate_arguments_before_the_gpu():
+    """Bad arguments come back as status codes before any CUDA call (so these run without a
+    GPU): null or empty inputs and out-of-range indices as GSLAM_ERR_BAD_INPUT, sizes past a
+    fixed capacity as GSLAM_ERR_TOO_LARGE, each with a message in gslam_last_error."""
+    G = load_pkg()
+    A = G.abi
+    L = A.lib()
+    out = C.c_void_p()
+    one = np.zeros(3)
+    idx = np.array([0, 7], np.uint32)
+    meas = np.zeros((2, 3))
+    se2 = lambda n, ei, ej, ne: A.SE2GraphDesc(n, A.ptr(one), ne, A.ptr(ei, C.c_uint32),  # noqa: E731
+                                               A.ptr(ej, C.c_uint32), A.ptr(meas), A.ptr(meas), 0.1, 1e6)
+    assert L.gslam_create_se2(None, None, C.byref(out)) == A.ERR_BAD_INPUT
+    assert L.gslam_create_se2(C.byref(se2(0, idx, idx, 0)), None, C.byref(out)) == A.ERR_BAD_INPUT
+    assert L.gslam_create_se2(C.byref(se2(5, idx, idx, 2)), None, C.byref(out)) == A.ERR_BAD_INPUT
+    assert b"out of range" in L.gslam_last_error()
+    assert L.gslam_create_se2(C.byref(se2(0x40000000, idx, idx, 0)), None, C.byref(out)) == A.ERR_TOO_LARGE
+    assert out.value is None
+    # a batch: a graph without poses, an edge out of range, a non-positive lambda
+    g_ok = se2(8, idx, idx, 2)
+    for bad in (se2(0, idx, idx, 0), se2(5, idx, idx, 2)):
+        arr = (A.SE2GraphDesc * 2)(g_ok, bad)
+        assert L.gslam_create_se2_batch(arr, 2, None, C.byref(out)) == A.ERR_BAD_INPUT
+    neg = se2(8, idx, idx, 2)
+    neg.lam = -1.0
+    assert L.gslam_create_se2_batch((A.SE2GraphDesc * 1)(neg), 1, None, C.byref(out)) == A.ERR_BAD_INPUT
+    assert b"lambda" in L.gslam_last_error()
+    assert L.gslam_create_se2_batch(None, 0, None, C.byref(out)) == A.ERR_BAD_INPUT
+    # the reference's factor family: an observation step past the poses
+    u = np.zeros((4, 2))
+    steps = np.array([9], np.uint32)
+    rd = A.ReferenceGraphDesc(4, A.ptr(np.zeros((4, 3))), A.ptr(u), 1.0, 1.0, A.ptr(np.zeros(4)), 1,
+                              A.ptr(steps, C.c_uint32), A.ptr(steps, C.c_uint32), A.ptr(np.zeros((1, 2))))
+    assert L.gslam_create_reference(C.byref(rd), None, C.byref(out)) == A.ERR_BAD_INPUT
+    # dense path and the allocation-free solve (pointers are never dereferenced)
+    dummy = C.c_void_p(16)
+    assert L.gslam_gj_inverse(0, dummy, 0, None, None) == A.ERR_BAD_INPUT
+    assert L.gslam_gj_solve(4, dummy, 2, dummy, dummy, None, None) == A.ERR_BAD_INPUT
+    assert L.gslam_pcg_solve_static(7, dummy, dummy, dummy, dummy, dummy, 1e-6, 10, None, None) == A.ERR_BAD_INPUT
+    assert L.gslam_pcg_solve_static(3 * 16385, dummy, dummy, dummy, dummy, dummy, 1e-6, 10, None,
+                                    None) == A.ERR_TOO_LARGE
+    assert b"16384" in L.gslam_last_error()
