@@ -212,7 +212,7 @@ def test_gn_fixed_point_direct(oracle):
 
 
 def test_dense_gj_run_vs_reference_gj_dump(oracle):
-    """The dense path (north-star item f): the oracle's run of the reference's Gauss-Jordan
+    """The dense Gauss-Jordan path: the oracle's run of the reference's Gauss-Jordan
     program (oracle.run_dense_gj: dense Omega, GJ inverse, dx = Omega^-1 xi, the program's
     stop rules) on victoria-park-100 at lambda 0.06 against the reference's own committed
     pose dump of that program (tests/golden/ref_vp100_gj_fp64.npz). The program inverts
